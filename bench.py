@@ -1,0 +1,407 @@
+#!/usr/bin/env python
+"""Benchmark of the equirectangular rasterizer: forward + backward of one 2048 x 1024 view over
+1,000,000 Gaussians per step (the reference's headline single-view workload).
+
+    python bench.py [--gpus N] [--steps K] [--warmup W] [--impl omnigs|reference]
+
+One process per GPU (torchrun for N > 1, NCCL).  Each rank renders and back-propagates its own
+view of the shared Gaussian set (weak scaling); for N > 1 the per-Gaussian gradients are summed
+across ranks every step with one NCCL all-reduce, as a data-parallel train step does.
+
+* value: views/s of the whole job, device-timed with CUDA events on the launching stream over K
+  steps (max over ranks), inputs resident in HBM.  Each step touches far more than the 126 MB L2
+  (the SH coefficients alone are 192 MB), so no flush is needed between steps.
+* e2e: the same metric through the reference-facing LibTorch API (RasterizeGaussiansCUDA +
+  RasterizeGaussiansBackwardCUDA), with every step copying its per-view inputs (camera, upstream
+  image gradient) from pinned host memory and the rendered image back to pinned host memory.  The
+  Gaussian parameters and their gradients stay on the device, as in the reference trainer.
+* roofline: per-kernel device times from the library's event timing, against the algorithmic bytes
+  of each stage; the dominant kernel is reported against MEASURED_PEAKS.json.
+* cpu_baseline: the FP64 oracle (multithreaded C++ restatement of the reference algorithm) on the
+  same view, on this host's cores.
+* --impl reference: the reference arm.  The reference's rasterizer is CUDA-only, so its CPU
+  implementation of the path is the FP64 oracle port, timed here on all host cores.
+"""
+from __future__ import annotations
+
+import argparse
+import json
+import math
+import os
+import statistics
+import subprocess
+import sys
+import threading
+import time
+
+import numpy as np
+
+ROOT = os.path.dirname(os.path.abspath(__file__))
+sys.path.insert(0, ROOT)
+
+METRIC = "fwd+bwd ms/view & views/s, 1M Gaussians 2048x1024 ERP, batched vs plain"
+UNIT = "views/s"
+P_GAUSS, WIDTH, HEIGHT = 1_000_000, 2048, 1024
+WORKLOAD = "plain single-view fwd+bwd, 1M Gaussians, 2048x1024 equirect, identity pose, SH deg 3"
+
+
+def parse():
+    ap = argparse.ArgumentParser()
+    ap.add_argument("--gpus", type=int, default=1)
+    ap.add_argument("--steps", type=int, default=20)
+    ap.add_argument("--warmup", type=int, default=5)
+    ap.add_argument("--impl", default="omnigs", choices=["omnigs", "reference"])
+    ap.add_argument("--no-cpu-baseline", action="store_true")
+    ap.add_argument("--no-e2e", action="store_true")
+    return ap.parse_args()
+
+
+def dist_env():
+    return int(os.environ.get("RANK", 0)), int(os.environ.get("WORLD_SIZE", 1)), \
+        int(os.environ.get("LOCAL_RANK", 0))
+
+
+# ---------------------------------------------------------------- clocks -----------------------
+class ClockSampler:
+    """Samples SM clock and throttle reasons with nvidia-smi while running."""
+
+    FIELDS = ("clocks.sm,clocks.max.sm,power.draw,clocks_event_reasons.active,"
+              "clocks_event_reasons.hw_slowdown,clocks_event_reasons.hw_thermal_slowdown,"
+              "clocks_event_reasons.sw_thermal_slowdown,clocks_event_reasons.sw_power_cap")
+
+    def __init__(self, gpu_id: str | None):
+        self.gpu_id, self.proc, self.lines = gpu_id, None, []
+
+    def __enter__(self):
+        cmd = ["nvidia-smi", f"--query-gpu={self.FIELDS}", "--format=csv,noheader,nounits", "-lms", "200"]
+        if self.gpu_id:
+            cmd += ["-i", self.gpu_id]
+        try:
+            self.proc = subprocess.Popen(cmd, stdout=subprocess.PIPE, stderr=subprocess.DEVNULL, text=True)
+            self.thread = threading.Thread(target=self._read, daemon=True)
+            self.thread.start()
+        except OSError:
+            self.proc = None
+        return self
+
+    def _read(self):
+        for line in self.proc.stdout:
+            self.lines.append(line.strip())
+
+    def __exit__(self, *exc):
+        if self.proc is not None:
+            self.proc.terminate()
+            try:
+                self.proc.wait(timeout=5)
+            except subprocess.TimeoutExpired:
+                self.proc.kill()
+
+    def summary(self) -> dict:
+        sm, mx, reasons = [], [], set()
+        names = ["hw_slowdown", "hw_thermal_slowdown", "sw_thermal_slowdown", "sw_power_cap"]
+        for ln in self.lines:
+            parts = [p.strip() for p in ln.split(",")]
+            if len(parts) < 8:
+                continue
+            try:
+                sm.append(float(parts[0]))
+                mx.append(float(parts[1]))
+            except ValueError:
+                continue
+            for n, v in zip(names, parts[4:8]):
+                if v.lower() == "active":
+                    reasons.add(n)
+        if not sm:
+            return {"sm_mhz": None, "sm_max_mhz": None, "reasons": ["unavailable"], "samples": 0}
+        return {"sm_mhz": statistics.median(sm), "sm_max_mhz": max(mx), "reasons": sorted(reasons),
+                "samples": len(sm)}
+
+
+# ---------------------------------------------------------------- roofline ---------------------
+def measured_peaks():
+    path = os.path.join(ROOT, "MEASURED_PEAKS.json")
+    if os.path.exists(path):
+        with open(path) as f:
+            d = json.load(f)
+        return float(d["hbm_gbs"]), float(d.get("sm_max_mhz", 1965.0)), "measured"
+    return 6650.0, 1965.0, "fallback"
+
+
+def traffic_from_profiles() -> dict:
+    """Per-launch DRAM bytes per kernel from the committed ncu summary, if present."""
+    path = os.path.join(ROOT, "profiles", "dram_traffic_per_launch.txt")
+    out = {}
+    if os.path.exists(path):
+        for ln in open(path):
+            parts = ln.split()
+            if len(parts) >= 2 and not ln.startswith("#"):
+                try:
+                    out[parts[0]] = float(parts[1])
+                except ValueError:
+                    pass
+    return out
+
+
+def stage_bytes(P, V, R, N, Tl):
+    """Algorithmic (compulsory) HBM bytes of each stage for one view."""
+    return {
+        "preprocess": 44 * P + 192 * V + 8 * P + 40 * V + 8 * P,  # + the fused scan of tiles_touched
+        "duplicate": 20 * V + 12 * R,
+        "sort": 24 * R,
+        "ranges": 8 * R + 8 * Tl,
+        "render_forward": 40 * R + 8 * Tl + 12 * N + 8 * N,
+        "render_backward": 40 * R + 8 * Tl + 12 * N + 8 * N + 44 * V,
+        "preprocess_backward": 264 * V + 232 * V,
+    }
+
+
+# ---------------------------------------------------------------- CPU baseline ------------------
+def cpu_baseline(g, view, dpix_np, budget_s=30.0):
+    import oracle
+    nthreads = os.cpu_count() or 1
+    t0 = time.perf_counter()
+    oracle.forward_backward(g, view, dpix_np, nthreads=nthreads)
+    t = time.perf_counter() - t0
+    reps = 1
+    if 2 * t < budget_s:
+        t0 = time.perf_counter()
+        reps = max(1, min(5, int(budget_s / max(t, 1e-3)) - 1))
+        for _ in range(reps):
+            oracle.forward_backward(g, view, dpix_np, nthreads=nthreads)
+        t = (time.perf_counter() - t0) / reps
+    return {"value": 1.0 / t, "unit": UNIT, "cores": nthreads, "kind": "port",
+            "sample": f"{reps} full view(s) of the headline workload (1M Gaussians, 2048x1024, "
+                      f"fwd+bwd) through the FP64 oracle; {t:.2f} s per view"}
+
+
+# ---------------------------------------------------------------- reference arm ----------------
+def run_reference(args, rank, world):
+    if rank != 0:
+        return
+    from omnigs_b200 import scenes
+    g = scenes.make_gaussians(P_GAUSS, seed=0)
+    view = scenes.identity_view(WIDTH, HEIGHT)
+    dpix = scenes.upstream_grad(WIDTH, HEIGHT)
+    import oracle
+    nthreads = os.cpu_count() or 1
+    t0 = time.perf_counter()
+    if args.warmup > 0:
+        oracle.forward_backward(g, view, dpix, nthreads=nthreads)
+    t_est = max(time.perf_counter() - t0, 1e-3)
+    steps = max(1, min(args.steps, int(150.0 / t_est)))
+    t0 = time.perf_counter()
+    for _ in range(steps):
+        oracle.forward_backward(g, view, dpix, nthreads=nthreads)
+    dt = time.perf_counter() - t0
+    value = steps / dt
+    line = {"metric": METRIC, "value": value, "unit": UNIT, "n_gpus": world, "steps": steps,
+            "warmup": min(args.warmup, 1), "ms_per_step": 1000 * dt / steps, "higher_is_better": True,
+            "scaling": "weak", "vs_baseline": None, "dtype": "f64", "data": "synthetic (seeded scene generators)",
+            "config": {"workload": WORKLOAD, "gaussians": P_GAUSS, "width": WIDTH, "height": HEIGHT},
+            "impl": "reference",
+            "cpu_baseline": {"value": value, "unit": UNIT, "cores": nthreads, "kind": "port",
+                             "sample": f"{steps} full view(s); the reference rasterizer has no CPU "
+                                       "path, so this is the FP64 oracle restating its algorithm"},
+            "e2e": {"value": value, "unit": UNIT, "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0}}
+    print(json.dumps(line), flush=True)
+
+
+# ---------------------------------------------------------------- omnigs arm --------------------
+def run_omnigs(args, rank, world, local_rank):
+    import torch
+    import torch.distributed as dist
+
+    from omnigs_b200 import capi, lonlat, scenes, torch_ext
+
+    dev = torch.device("cuda", local_rank)
+    torch.cuda.set_device(dev)
+    g = scenes.make_gaussians(P_GAUSS, seed=0)
+    view = scenes.identity_view(WIDTH, HEIGHT)
+    dpix_np = scenes.upstream_grad(WIDTH, HEIGHT, seed=2 + rank)
+    gt = lonlat.GaussianTensors.from_numpy(g, dev)
+    cam = lonlat.Camera.from_view(view, dev)
+    dpix = torch.from_numpy(dpix_np).to(dev)
+    P, W, H = g.P, WIDTH, HEIGHT
+
+    # sizing pass (untimed): exact instance count, then a fixed capacity for the timed steps
+    _, radii0, n0, _ = lonlat.rasterize(gt, cam)
+    V = int((radii0 > 0).sum())
+    capacity = n0 + n0 // 8 + 4096
+    state = lonlat.LonlatState(P, W, H, capacity, dev)
+    out = torch.empty(3, H, W, device=dev)
+    radii = torch.empty(P, dtype=torch.int32, device=dev)
+    # one flat buffer holds every gradient output, so N > 1 reduces it with a single all-reduce
+    sizes = [P * 3, P * 3, P, P * 3, P * 6, P * 16 * 3, P * 3, P * 4]
+    flat = torch.empty(sum(sizes), device=dev)
+    parts = torch.split(flat, sizes)
+    grads = lonlat.Gradients(parts[0].view(P, 3), parts[1].view(P, 3), parts[2].view(P, 1),
+                             parts[3].view(P, 3), parts[4].view(P, 6), parts[5].view(P, 16, 3),
+                             parts[6].view(P, 3), parts[7].view(P, 4))
+
+    def step():
+        state.forward(gt, cam, out, radii)
+        state.backward(gt, cam, radii, dpix, grads)
+        if world > 1:
+            dist.all_reduce(flat)
+
+    for _ in range(args.warmup):
+        step()
+    torch.cuda.synchronize()
+    nr, st = state.status()
+    assert st == 0 and nr == n0, (nr, st)
+
+    gpu_uuid = None
+    try:
+        gpu_uuid = "GPU-" + str(torch.cuda.get_device_properties(dev).uuid)
+    except Exception:
+        pass
+    stream = torch.cuda.current_stream(dev)
+    ev0, ev1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+    if world > 1:
+        dist.barrier()
+    torch.cuda.synchronize()
+    launches0 = capi.kernel_launches()
+    with ClockSampler(gpu_uuid) as clocks:
+        ev0.record(stream)
+        for _ in range(args.steps):
+            step()
+        ev1.record(stream)
+        torch.cuda.synchronize()
+    launches = capi.kernel_launches() - launches0
+    if world > 1:
+        dist.barrier()
+    ms_total = ev0.elapsed_time(ev1)
+    if world > 1:
+        t = torch.tensor([ms_total], device=dev)
+        dist.all_reduce(t, op=dist.ReduceOp.MAX)
+        ms_total = float(t.item())
+    ms_per_step = ms_total / args.steps
+    value = world * args.steps / (ms_total / 1000.0)
+
+    # ---- per-kernel device times (library event timing) for the roofline ----
+    capi.timing_enable(True)
+    for _ in range(args.steps):
+        step()
+    torch.cuda.synchronize()
+    stages = capi.timing_read()
+    capi.timing_enable(False)
+    iv = state.image_view()
+    pairs_bwd = int(iv["n_contrib"].to(torch.int64).sum())
+    Tl = ((W + 15) // 16) * ((H + 15) // 16)
+    sbytes = stage_bytes(P, V, n0, W * H, Tl)
+    hbm_peak, sm_max_mhz, peak_kind = measured_peaks()
+    traffic = traffic_from_profiles()
+    kernels = {}
+    for name, nbytes in sbytes.items():
+        ms, nl = stages[name]
+        if nl == 0:
+            continue
+        per_step_ms = ms / args.steps
+        kernels[name] = {"ms_per_step": round(per_step_ms, 4), "launches_per_step": nl // args.steps,
+                         "algorithmic_bytes": nbytes, "GBps": round(nbytes / (per_step_ms * 1e-3) / 1e9, 1)}
+    dominant = max(kernels, key=lambda k: kernels[k]["ms_per_step"])
+    dk = kernels[dominant]
+    launch_ms = stages[dominant][0] / max(stages[dominant][1], 1)
+    bytes_per_launch = sbytes[dominant] / max(dk["launches_per_step"], 1)
+    achieved = bytes_per_launch / (launch_ms * 1e-3) / 1e9
+    roofline = {"bound": "hbm", "kernel": dominant, "achieved": round(achieved, 1), "peak": hbm_peak,
+                "unit": "GB/s", "frac": round(achieved / hbm_peak, 4),
+                "traffic": traffic.get(dominant), "peak_source": f"{peak_kind} (MEASURED_PEAKS.json hbm_gbs)"}
+    fp32_peak = 148 * 128 * 2 * sm_max_mhz * 1e6 / 1e12
+    flops_fwd = pairs_bwd * 24
+    flops_bwd = pairs_bwd * 64
+    rf = {}
+    for k, fl in (("render_forward", flops_fwd), ("render_backward", flops_bwd)):
+        if k in kernels:
+            tf = fl / (kernels[k]["ms_per_step"] * 1e-3) / 1e12
+            rf[k] = {"achieved_tflops": round(tf, 2), "frac": round(tf / fp32_peak, 4), "pairs": pairs_bwd,
+                     "flops_per_pair": 24 if k == "render_forward" else 64}
+    roofline_fp32 = {"bound": "fp32", "peak_tflops": round(fp32_peak, 1),
+                     "peak_source": "nominal 148 SM x 128 FP32 lanes x 2 x sm_max_mhz", **rf}
+
+    # ---- end to end through the reference-facing LibTorch API with host buffers ----
+    e2e = None
+    if not args.no_e2e:
+        ext = torch_ext()
+        h_dpix = torch.from_numpy(dpix_np).pin_memory()
+        h_view = torch.from_numpy(view.viewmatrix).pin_memory()
+        h_campos = torch.from_numpy(view.campos).pin_memory()
+        h_bg = torch.zeros(3).pin_memory()
+        h_img = torch.empty(3, H, W).pin_memory()
+        empty = torch.empty(0, device=dev)
+        d_dpix = torch.empty_like(dpix)
+        d_view, d_campos, d_bg = (torch.empty(4, 4, device=dev), torch.empty(3, device=dev),
+                                  torch.empty(3, device=dev))
+
+        def e2e_step():
+            d_dpix.copy_(h_dpix, non_blocking=True)
+            d_view.copy_(h_view, non_blocking=True)
+            d_campos.copy_(h_campos, non_blocking=True)
+            d_bg.copy_(h_bg, non_blocking=True)
+            n, color, rad, gb, bb, ib = ext.rasterize_gaussians_cuda(
+                d_bg, gt.means3D, empty, gt.opacities, gt.scales, gt.rotations, 1.0, empty, d_view, d_view,
+                0.0, 0.0, H, W, gt.shs, 3, d_campos, False, 3, False)
+            ext.rasterize_gaussians_backward_cuda(
+                d_bg, gt.means3D, rad, empty, gt.scales, gt.rotations, 1.0, empty, d_view, d_view, 0.0, 0.0,
+                d_dpix, gt.shs, 3, d_campos, gb, n, bb, ib, 3)
+            h_img.copy_(color, non_blocking=True)
+
+        for _ in range(max(2, args.warmup)):
+            e2e_step()
+        torch.cuda.synchronize()
+        if world > 1:
+            dist.barrier()
+        e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+        e0.record(stream)
+        for _ in range(args.steps):
+            e2e_step()
+        e1.record(stream)
+        torch.cuda.synchronize()
+        ems = e0.elapsed_time(e1)
+        if world > 1:
+            t = torch.tensor([ems], device=dev)
+            dist.all_reduce(t, op=dist.ReduceOp.MAX)
+            ems = float(t.item())
+        e2e = {"value": world * args.steps / (ems / 1000.0), "unit": UNIT,
+               "h2d_bytes_per_step": int(h_dpix.numel() * 4 + 16 * 4 + 3 * 4 + 3 * 4),
+               "d2h_bytes_per_step": int(h_img.numel() * 4 + 4),
+               "api": "RasterizeGaussiansCUDA + RasterizeGaussiansBackwardCUDA (LibTorch layer)"}
+
+    cpu = None
+    if rank == 0 and world == 1 and not args.no_cpu_baseline:
+        cpu = cpu_baseline(g, view, dpix_np)
+
+    if rank == 0:
+        line = {"metric": METRIC, "value": round(value, 3), "unit": UNIT, "n_gpus": world,
+                "steps": args.steps, "warmup": args.warmup, "ms_per_step": round(ms_per_step, 4),
+                "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "f32",
+                "data": "synthetic (seeded generators of the reference's config shapes)",
+                "config": {"workload": WORKLOAD, "gaussians": P, "width": W, "height": H,
+                           "num_rendered": n0, "visible": V, "parallelism": f"dp{world} (views)",
+                           "l2": "inputs larger than L2 (SH alone 192 MB > 126 MB), no flush"},
+                "gpu_launches": int(launches), "clocks": clocks.summary(), "roofline": roofline,
+                "roofline_fp32": roofline_fp32, "kernels": kernels, "e2e": e2e, "cpu_baseline": cpu}
+        print(json.dumps(line), flush=True)
+
+
+def main():
+    args = parse()
+    rank, world, local_rank = dist_env()
+    if args.impl == "reference":
+        run_reference(args, rank, world)
+        return
+    if world > 1:
+        import datetime
+
+        import torch.distributed as dist
+        dist.init_process_group("nccl", timeout=datetime.timedelta(seconds=120))
+    try:
+        run_omnigs(args, rank, world, local_rank)
+    finally:
+        if world > 1:
+            import torch.distributed as dist
+            dist.destroy_process_group()
+
+
+if __name__ == "__main__":
+    main()

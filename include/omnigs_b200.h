@@ -1,0 +1,208 @@
+/* omnigs_b200 -- B200-native equirectangular (lonlat) differentiable Gaussian rasterizer, C ABI.
+ *
+ * This is the drop-in boundary for OmniGS's camera_type = 3 path.  Every entry point takes plain
+ * device pointers, sizes and a CUDA stream; no torch types cross it.  The LibTorch layer in
+ * omnigs_b200/csrc/torch re-exports the reference's unchanged C++ surface on top of it:
+ *
+ *   RasterizeGaussiansCUDA          (src/rasterize_points.cu:49-164, include/rasterize_points.h:29-50)
+ *   RasterizeGaussiansBackwardCUDA  (src/rasterize_points.cu:166-285, include/rasterize_points.h:52-74)
+ *   markVisible                     (src/rasterize_points.cu:287-319, include/rasterize_points.h:76-80)
+ *
+ * Array conventions are the reference's: means3D [P,3], scales [P,3] (activated), rotations [P,4]
+ * (r, x, y, z; used as given, not normalised), opacities [P] (activated), shs [P,M,3]
+ * (coefficient-major, RGB inner), viewmatrix [16] = Tcw stored column-major (the row-major
+ * storage of world_view_transform = Tcw^T), campos [3], background [3], images [3,H,W].
+ * Optional inputs are NULL, as the reference's empty tensors are.
+ *
+ * The three state buffers (geometry, binning, image) are caller-owned device memory whose sizes
+ * come from the *_bytes queries; their layout is private to this library.  Nothing here allocates
+ * device memory and nothing synchronises the host except omnigs_lonlat_read_status.  The instance
+ * count (num_rendered) is produced and consumed on the device; the binning buffer is sized for a
+ * caller-chosen capacity and a pass that would exceed it does no binning work and reports
+ * OMNIGS_STATUS_CAPACITY through the status word.
+ *
+ * Return codes: 0 on success, otherwise one of OMNIGS_ERR_*; omnigs_last_error() gives a message
+ * (thread-local).  Kernels never trap: device-side failures are bits of the status word.
+ */
+#ifndef OMNIGS_B200_H_
+#define OMNIGS_B200_H_
+
+#include <stddef.h>
+#include <stdint.h>
+
+#ifdef __cplusplus
+extern "C" {
+#endif
+
+typedef struct CUstream_st* omnigs_stream_t; /* same type as cudaStream_t */
+
+#define OMNIGS_OK 0
+#define OMNIGS_ERR_INVALID_ARGUMENT 1
+#define OMNIGS_ERR_BUFFER_TOO_SMALL 2
+#define OMNIGS_ERR_CUDA 3
+#define OMNIGS_ERR_UNSUPPORTED 4
+#define OMNIGS_ERR_CAPACITY 5 /* num_rendered exceeds the binning capacity */
+#define OMNIGS_ERR_DEVICE 6   /* a device-side status bit other than capacity is set */
+
+/* Bits of the device status word (omnigs_lonlat_read_status). */
+#define OMNIGS_STATUS_CAPACITY 1u /* num_rendered > binning capacity: binning and blend skipped */
+#define OMNIGS_STATUS_LOOKBACK 2u /* a bounded cross-block wait gave up; results are invalid */
+#define OMNIGS_STATUS_OVERFLOW 4u /* more than 2^30 - 1 instances */
+
+#define OMNIGS_CAMERA_PINHOLE 1
+#define OMNIGS_CAMERA_LONLAT 3
+
+/* Inputs and outputs of one forward rasterization.
+ * Replaces the argument list of CudaRasterizer::LonlatRasterizer::forward
+ * (cuda_rasterizer/rasterizer.h:104-123) as called from src/rasterize_points.cu:136-155. */
+typedef struct OmnigsLonlatForwardArgs {
+  int P;                      /* number of Gaussians */
+  int D;                      /* active SH degree, 0..3 */
+  int M;                      /* SH coefficients per Gaussian (sh.size(1)); 0 without SH */
+  int W, H;                   /* equirect image size */
+  const float* background;    /* [3] */
+  const float* means3D;       /* [P,3] */
+  const float* shs;           /* [P,M,3] or NULL (then colors_precomp) */
+  const float* colors_precomp;/* [P,3] or NULL */
+  const float* opacities;     /* [P] */
+  const float* scales;        /* [P,3] or NULL (then cov3D_precomp) */
+  float scale_modifier;
+  const float* rotations;     /* [P,4] or NULL */
+  const float* cov3D_precomp; /* [P,6] or NULL */
+  const float* viewmatrix;    /* [16] */
+  const float* campos;        /* [3] */
+  float* out_color;           /* [3,H,W] output */
+  int* radii;                 /* [P] output */
+} OmnigsLonlatForwardArgs;
+
+/* Inputs and outputs of one backward pass.
+ * Replaces CudaRasterizer::LonlatRasterizer::backward (cuda_rasterizer/rasterizer.h:126-154) as
+ * called from src/rasterize_points.cu:249-276.  All outputs are fully written (zeros for
+ * Gaussians with radius 0); the caller does not need to clear them. */
+typedef struct OmnigsLonlatBackwardArgs {
+  int P, D, M, W, H;
+  int R;                      /* num_rendered of the forward, or -1 to use the device value */
+  const float* background;
+  const float* means3D;
+  const float* shs;
+  const float* colors_precomp;
+  const float* scales;
+  float scale_modifier;
+  const float* rotations;
+  const float* cov3D_precomp;
+  const float* viewmatrix;
+  const float* campos;
+  const int* radii;           /* [P], from the forward */
+  const float* dL_dout_color; /* [3,H,W] */
+  float* dL_dmeans2D;         /* [P,3] (viewspace-point gradient, NDC scale, z = 0) */
+  float* dL_dcolors;          /* [P,3] */
+  float* dL_dopacity;         /* [P] */
+  float* dL_dmeans3D;         /* [P,3] */
+  float* dL_dcov3D;           /* [P,6] */
+  float* dL_dsh;              /* [P,M,3] or NULL when M == 0 */
+  float* dL_dscales;          /* [P,3] */
+  float* dL_drotations;       /* [P,4] */
+  float* dL_dconic;           /* [P,4] (x, y, 0, w) or NULL; internal in the reference */
+} OmnigsLonlatBackwardArgs;
+
+/* Library version string. */
+const char* omnigs_version(void);
+
+/* Message of the last error on this host thread ("" if none). */
+const char* omnigs_last_error(void);
+
+/* Buffer sizes.  GeometryState / ImageState / BinningState sizes of the reference
+ * (rasterizer_impl.h:97-102, required<T>); the binning size is a function of the capacity, the
+ * largest num_rendered it can hold. */
+size_t omnigs_lonlat_geom_bytes(int P);
+size_t omnigs_lonlat_image_bytes(int W, int H);
+size_t omnigs_lonlat_binning_bytes(int64_t capacity);
+int64_t omnigs_lonlat_binning_capacity(size_t binning_bytes);
+
+/* Preprocess + scan (forward.cu:592-703 and rasterizer_impl.cu:622-623): writes radii and the
+ * geometry buffer, including the device-side num_rendered.  No host synchronisation. */
+int omnigs_lonlat_preprocess(const OmnigsLonlatForwardArgs* args, void* geom, size_t geom_bytes,
+                             omnigs_stream_t stream);
+
+/* Binning + forward blend (rasterizer_impl.cu:630-694): duplicate keys, radix sort, tile ranges,
+ * blend into out_color.  Resumes from a geometry buffer filled by omnigs_lonlat_preprocess, so a
+ * caller whose binning capacity was too small can resize and call this again. */
+int omnigs_lonlat_render(const OmnigsLonlatForwardArgs* args, void* geom, size_t geom_bytes,
+                         void* binning, size_t binning_bytes, void* image, size_t image_bytes,
+                         omnigs_stream_t stream);
+
+/* omnigs_lonlat_preprocess followed by omnigs_lonlat_render.  Replaces
+ * CudaRasterizer::LonlatRasterizer::forward (rasterizer_impl.cu:540-697) without its mid-pass
+ * device-to-host copy of num_rendered (:627-628). */
+int omnigs_lonlat_forward(const OmnigsLonlatForwardArgs* args, void* geom, size_t geom_bytes,
+                          void* binning, size_t binning_bytes, void* image, size_t image_bytes,
+                          omnigs_stream_t stream);
+
+/* Waits for `stream` and copies num_rendered and the status word to the host.  The one call that
+ * synchronises; the reference's forward returns num_rendered by value (rasterizer.h:104). */
+int omnigs_lonlat_read_status(const void* geom, int* num_rendered, uint32_t* status,
+                              omnigs_stream_t stream);
+
+/* Backward blend + backward preprocess.  Replaces CudaRasterizer::LonlatRasterizer::backward
+ * (rasterizer_impl.cu:701-795). */
+int omnigs_lonlat_backward(const OmnigsLonlatBackwardArgs* args, void* geom, size_t geom_bytes,
+                           const void* binning, size_t binning_bytes, const void* image,
+                           size_t image_bytes, omnigs_stream_t stream);
+
+/* Visibility marks.  camera_type 3: every Gaussian (markAllVisible, rasterizer_impl.cu:82-90);
+ * camera_type 1: the pinhole near test p_view.z > 0.2 (checkFrustum, rasterizer_impl.cu:66-78,
+ * auxiliary.h:166-196).  present is a [P] byte array. */
+int omnigs_mark_visible(int P, const float* means3D, const float* viewmatrix, int camera_type,
+                        uint8_t* present, omnigs_stream_t stream);
+
+/* Per-stage device timing.  While enabled, every kernel this library launches is bracketed by
+ * CUDA events recorded on its launch stream; omnigs_timing_read waits for the recorded events and
+ * returns the summed device time and launch count per stage since the last read.  Disabled by
+ * default (no events are recorded).  The reference has only host chrono timing
+ * (src/gaussian_mapper.cpp:293, 738-781). */
+#define OMNIGS_STAGE_PREPROCESS 0
+#define OMNIGS_STAGE_DUPLICATE 1
+#define OMNIGS_STAGE_SORT 2
+#define OMNIGS_STAGE_RANGES 3
+#define OMNIGS_STAGE_RENDER_FORWARD 4
+#define OMNIGS_STAGE_RENDER_BACKWARD 5
+#define OMNIGS_STAGE_PREPROCESS_BACKWARD 6
+#define OMNIGS_STAGE_OTHER 7
+#define OMNIGS_NUM_STAGES 8
+typedef struct OmnigsStageTimes {
+  double ms[OMNIGS_NUM_STAGES];
+  uint64_t launches[OMNIGS_NUM_STAGES];
+} OmnigsStageTimes;
+int omnigs_timing_enable(int enable);
+int omnigs_timing_read(OmnigsStageTimes* out);
+
+/* Number of kernels this library has launched since it was loaded. */
+uint64_t omnigs_kernel_launches(void);
+
+/* Read-only views into the private buffers, for inspection and parity testing.  Pointers are
+ * device pointers inside the given buffers. */
+typedef struct OmnigsLonlatGeomView {
+  const float* splat;       /* [P][8]: x, y, conic a, conic b, conic c, opacity, cull hx, cull hy */
+  const float* color;       /* [P][4]: r, g, b, clamp bits (as uint32) */
+  const float* depth;       /* [P] radial distance r */
+  const uint32_t* offsets;  /* [P] inclusive scan of tiles_touched */
+} OmnigsLonlatGeomView;
+typedef struct OmnigsLonlatBinningView {
+  const uint64_t* keys;     /* [num_rendered] sorted tile|depth keys */
+  const uint32_t* point_list; /* [num_rendered] sorted Gaussian indices */
+} OmnigsLonlatBinningView;
+typedef struct OmnigsLonlatImageView {
+  const float* final_T;     /* [H*W] */
+  const uint32_t* n_contrib;/* [H*W] last contributor (1-based position in the tile range) */
+  const uint32_t* ranges;   /* [tiles][2] */
+} OmnigsLonlatImageView;
+int omnigs_lonlat_geom_view(const void* geom, int P, OmnigsLonlatGeomView* out);
+int omnigs_lonlat_binning_view(const void* binning, size_t binning_bytes, int W, int H,
+                               OmnigsLonlatBinningView* out);
+int omnigs_lonlat_image_view(const void* image, int W, int H, OmnigsLonlatImageView* out);
+
+#ifdef __cplusplus
+}
+#endif
+
+#endif /* OMNIGS_B200_H_ */

@@ -1,0 +1,168 @@
+"""ctypes binding of the C ABI in include/omnigs_b200.h (libomnigs_b200.so).
+
+The functions here take torch CUDA tensors, pass their device pointers and the current CUDA
+stream through the C ABI, and raise on a non-zero return code.  There is no CPU path: if the
+library is missing this module raises instead of falling back.
+"""
+from __future__ import annotations
+
+import ctypes
+import os
+
+import torch
+
+_HERE = os.path.dirname(os.path.abspath(__file__))
+LIB_PATH = os.path.join(_HERE, "lib", "libomnigs_b200.so")
+
+OMNIGS_OK = 0
+ERR_NAMES = {1: "INVALID_ARGUMENT", 2: "BUFFER_TOO_SMALL", 3: "CUDA", 4: "UNSUPPORTED",
+             5: "CAPACITY", 6: "DEVICE"}
+STATUS_CAPACITY = 1
+STATUS_LOOKBACK = 2
+STATUS_OVERFLOW = 4
+CAMERA_PINHOLE = 1
+CAMERA_LONLAT = 3
+
+_vp = ctypes.c_void_p
+_i = ctypes.c_int
+_f = ctypes.c_float
+
+
+class ForwardArgs(ctypes.Structure):
+    _fields_ = [("P", _i), ("D", _i), ("M", _i), ("W", _i), ("H", _i),
+                ("background", _vp), ("means3D", _vp), ("shs", _vp), ("colors_precomp", _vp),
+                ("opacities", _vp), ("scales", _vp), ("scale_modifier", _f), ("rotations", _vp),
+                ("cov3D_precomp", _vp), ("viewmatrix", _vp), ("campos", _vp),
+                ("out_color", _vp), ("radii", _vp)]
+
+
+class BackwardArgs(ctypes.Structure):
+    _fields_ = [("P", _i), ("D", _i), ("M", _i), ("W", _i), ("H", _i), ("R", _i),
+                ("background", _vp), ("means3D", _vp), ("shs", _vp), ("colors_precomp", _vp),
+                ("scales", _vp), ("scale_modifier", _f), ("rotations", _vp), ("cov3D_precomp", _vp),
+                ("viewmatrix", _vp), ("campos", _vp), ("radii", _vp), ("dL_dout_color", _vp),
+                ("dL_dmeans2D", _vp), ("dL_dcolors", _vp), ("dL_dopacity", _vp),
+                ("dL_dmeans3D", _vp), ("dL_dcov3D", _vp), ("dL_dsh", _vp), ("dL_dscales", _vp),
+                ("dL_drotations", _vp), ("dL_dconic", _vp)]
+
+
+STAGES = ["preprocess", "duplicate", "sort", "ranges", "render_forward", "render_backward",
+          "preprocess_backward", "other"]
+
+
+class StageTimes(ctypes.Structure):
+    _fields_ = [("ms", ctypes.c_double * 8), ("launches", ctypes.c_uint64 * 8)]
+
+
+class GeomView(ctypes.Structure):
+    _fields_ = [("splat", _vp), ("color", _vp), ("depth", _vp), ("offsets", _vp)]
+
+
+class BinningView(ctypes.Structure):
+    _fields_ = [("keys", _vp), ("point_list", _vp)]
+
+
+class ImageView(ctypes.Structure):
+    _fields_ = [("final_T", _vp), ("n_contrib", _vp), ("ranges", _vp)]
+
+
+# every symbol include/omnigs_b200.h declares
+EXPORTED = ["omnigs_version", "omnigs_last_error", "omnigs_lonlat_geom_bytes",
+            "omnigs_lonlat_image_bytes", "omnigs_lonlat_binning_bytes",
+            "omnigs_lonlat_binning_capacity", "omnigs_lonlat_preprocess", "omnigs_lonlat_render",
+            "omnigs_lonlat_forward", "omnigs_lonlat_read_status", "omnigs_lonlat_backward",
+            "omnigs_mark_visible", "omnigs_timing_enable", "omnigs_timing_read",
+            "omnigs_kernel_launches", "omnigs_lonlat_geom_view", "omnigs_lonlat_binning_view",
+            "omnigs_lonlat_image_view"]
+
+_lib = None
+
+
+def lib() -> ctypes.CDLL:
+    """Load libomnigs_b200.so (raises if it has not been built)."""
+    global _lib
+    if _lib is None:
+        if not os.path.exists(LIB_PATH):
+            raise ImportError(f"{LIB_PATH} is missing; build it with `python -m omnigs_b200.build`")
+        L = ctypes.CDLL(LIB_PATH)
+        L.omnigs_version.restype = ctypes.c_char_p
+        L.omnigs_last_error.restype = ctypes.c_char_p
+        L.omnigs_lonlat_geom_bytes.restype = ctypes.c_size_t
+        L.omnigs_lonlat_geom_bytes.argtypes = [_i]
+        L.omnigs_lonlat_image_bytes.restype = ctypes.c_size_t
+        L.omnigs_lonlat_image_bytes.argtypes = [_i, _i]
+        L.omnigs_lonlat_binning_bytes.restype = ctypes.c_size_t
+        L.omnigs_lonlat_binning_bytes.argtypes = [ctypes.c_int64]
+        L.omnigs_lonlat_binning_capacity.restype = ctypes.c_int64
+        L.omnigs_lonlat_binning_capacity.argtypes = [ctypes.c_size_t]
+        fw = [ctypes.POINTER(ForwardArgs), _vp, ctypes.c_size_t]
+        L.omnigs_lonlat_preprocess.argtypes = fw + [_vp]
+        L.omnigs_lonlat_render.argtypes = fw + [_vp, ctypes.c_size_t, _vp, ctypes.c_size_t, _vp]
+        L.omnigs_lonlat_forward.argtypes = fw + [_vp, ctypes.c_size_t, _vp, ctypes.c_size_t, _vp]
+        L.omnigs_lonlat_read_status.argtypes = [_vp, ctypes.POINTER(_i),
+                                                ctypes.POINTER(ctypes.c_uint32), _vp]
+        L.omnigs_lonlat_backward.argtypes = [ctypes.POINTER(BackwardArgs), _vp, ctypes.c_size_t,
+                                             _vp, ctypes.c_size_t, _vp, ctypes.c_size_t, _vp]
+        L.omnigs_mark_visible.argtypes = [_i, _vp, _vp, _i, _vp, _vp]
+        L.omnigs_timing_enable.argtypes = [_i]
+        L.omnigs_timing_read.argtypes = [ctypes.POINTER(StageTimes)]
+        L.omnigs_kernel_launches.restype = ctypes.c_uint64
+        L.omnigs_lonlat_geom_view.argtypes = [_vp, _i, ctypes.POINTER(GeomView)]
+        L.omnigs_lonlat_binning_view.argtypes = [_vp, ctypes.c_size_t, _i, _i,
+                                                 ctypes.POINTER(BinningView)]
+        L.omnigs_lonlat_image_view.argtypes = [_vp, _i, _i, ctypes.POINTER(ImageView)]
+        _lib = L
+    return _lib
+
+
+class OmnigsError(RuntimeError):
+    pass
+
+
+def check(rc: int, what: str):
+    if rc != OMNIGS_OK:
+        msg = lib().omnigs_last_error().decode()
+        raise OmnigsError(f"{what} failed: {ERR_NAMES.get(rc, rc)}: {msg}")
+
+
+def ptr(t: torch.Tensor | None):
+    if t is None or t.numel() == 0:
+        return None
+    assert t.is_cuda and t.is_contiguous(), "C-ABI arguments must be contiguous CUDA tensors"
+    return t.data_ptr()
+
+
+def stream_handle(stream: torch.cuda.Stream | None = None):
+    s = stream if stream is not None else torch.cuda.current_stream()
+    return s.cuda_stream
+
+
+def geom_bytes(P: int) -> int:
+    return int(lib().omnigs_lonlat_geom_bytes(P))
+
+
+def image_bytes(W: int, H: int) -> int:
+    return int(lib().omnigs_lonlat_image_bytes(W, H))
+
+
+def binning_bytes(capacity: int) -> int:
+    return int(lib().omnigs_lonlat_binning_bytes(capacity))
+
+
+def binning_capacity(nbytes: int) -> int:
+    return int(lib().omnigs_lonlat_binning_capacity(nbytes))
+
+
+def timing_enable(on: bool):
+    lib().omnigs_timing_enable(1 if on else 0)
+
+
+def timing_read() -> dict:
+    """{stage: (total_ms, launches)} since the last read (waits for the recorded events)."""
+    t = StageTimes()
+    check(lib().omnigs_timing_read(ctypes.byref(t)), "omnigs_timing_read")
+    return {name: (float(t.ms[i]), int(t.launches[i])) for i, name in enumerate(STAGES)}
+
+
+def kernel_launches() -> int:
+    return int(lib().omnigs_kernel_launches())

@@ -1,0 +1,490 @@
+// C-ABI entry points (include/omnigs_b200.h): argument validation, buffer carving and kernel
+// sequencing for one lonlat rasterization.  Replaces the host orchestration of
+// CudaRasterizer::LonlatRasterizer (rasterizer_impl.cu:540-795) without its mid-pass host sync.
+#include <atomic>
+#include <cstdio>
+#include <cstring>
+#include <mutex>
+#include <string>
+#include <vector>
+
+#include "../../include/omnigs_b200.h"
+#include "kernels.h"
+
+namespace omnigs {
+namespace {
+
+thread_local std::string g_last_error;
+
+int fail(int code, const char* msg) {
+  g_last_error = msg;
+  return code;
+}
+
+int check_launch(const char* what) {
+  const cudaError_t e = cudaGetLastError();
+  if (e != cudaSuccess) {
+    g_last_error = std::string(what) + ": " + cudaGetErrorString(e);
+    return OMNIGS_ERR_CUDA;
+  }
+  return OMNIGS_OK;
+}
+
+template <class T>
+T* at(void* base, size_t off) {
+  return reinterpret_cast<T*>(static_cast<unsigned char*>(base) + off);
+}
+template <class T>
+const T* at(const void* base, size_t off) {
+  return reinterpret_cast<const T*>(static_cast<const unsigned char*>(base) + off);
+}
+
+// ---- launch accounting and optional per-stage event timing ----
+std::atomic<uint64_t> g_launches{0};
+std::atomic<bool> g_timing{false};
+std::mutex g_timing_mu;
+struct TimedLaunch {
+  int stage;
+  int kernels;
+  cudaEvent_t start, stop;
+};
+std::vector<TimedLaunch> g_timed;
+std::vector<cudaEvent_t> g_event_pool;
+
+cudaEvent_t take_event() {
+  if (!g_event_pool.empty()) {
+    cudaEvent_t e = g_event_pool.back();
+    g_event_pool.pop_back();
+    return e;
+  }
+  cudaEvent_t e = nullptr;
+  cudaEventCreate(&e);
+  return e;
+}
+
+// Runs `launch` (which enqueues `kernels` kernels on `s`) and accounts for it.
+template <class F>
+void staged(int stage, int kernels, cudaStream_t s, F&& launch) {
+  g_launches.fetch_add((uint64_t)kernels, std::memory_order_relaxed);
+  if (!g_timing.load(std::memory_order_relaxed)) {
+    launch();
+    return;
+  }
+  std::lock_guard<std::mutex> lock(g_timing_mu);
+  TimedLaunch t{stage, kernels, take_event(), take_event()};
+  cudaEventRecord(t.start, s);
+  launch();
+  cudaEventRecord(t.stop, s);
+  g_timed.push_back(t);
+}
+
+int sort_passes(int W, int H) {
+  const uint32_t tiles = (uint32_t)tiles_x(W) * (uint32_t)tiles_y(H);
+  const int bits = 32 + (int)higher_msb(tiles);
+  return (bits + kRadixBits - 1) / kRadixBits;
+}
+
+int validate_common(int P, int D, int M, int W, int H, const float* shs, const float* colors,
+                    const float* scales, const float* rotations, const float* cov3D,
+                    const float* means3D, const float* viewmatrix, const float* campos) {
+  if (P < 0) return fail(OMNIGS_ERR_INVALID_ARGUMENT, "P must be >= 0");
+  if (W <= 0 || H <= 0 || W > 65536 || H > 65536 || (int64_t)W * H > (int64_t(1) << 28))
+    return fail(OMNIGS_ERR_INVALID_ARGUMENT, "image size must be positive and at most 2^28 pixels");
+  if (P == 0) return OMNIGS_OK;
+  if (D < 0 || D > 3) return fail(OMNIGS_ERR_INVALID_ARGUMENT, "SH degree must be in [0, 3]");
+  if ((shs == nullptr) == (colors == nullptr))
+    return fail(OMNIGS_ERR_INVALID_ARGUMENT, "Please provide excatly one of either SHs or precomputed colors!");
+  if (shs != nullptr && M < (D + 1) * (D + 1))
+    return fail(OMNIGS_ERR_INVALID_ARGUMENT, "sh has fewer coefficients per Gaussian than the SH degree needs");
+  const bool have_sr = scales != nullptr || rotations != nullptr;
+  if ((have_sr && cov3D != nullptr) || (!have_sr && cov3D == nullptr) ||
+      (have_sr && (scales == nullptr || rotations == nullptr)))
+    return fail(OMNIGS_ERR_INVALID_ARGUMENT,
+                "Please provide exactly one of either scale/rotation pair or precomputed 3D covariance!");
+  if (means3D == nullptr || viewmatrix == nullptr || (shs != nullptr && campos == nullptr))
+    return fail(OMNIGS_ERR_INVALID_ARGUMENT, "means3D, viewmatrix and campos are required");
+  return OMNIGS_OK;
+}
+
+int validate_forward(const OmnigsLonlatForwardArgs* a) {
+  if (a == nullptr) return fail(OMNIGS_ERR_INVALID_ARGUMENT, "args is NULL");
+  const int rc = validate_common(a->P, a->D, a->M, a->W, a->H, a->shs, a->colors_precomp, a->scales,
+                                 a->rotations, a->cov3D_precomp, a->means3D, a->viewmatrix, a->campos);
+  if (rc) return rc;
+  if (a->out_color == nullptr || a->background == nullptr)
+    return fail(OMNIGS_ERR_INVALID_ARGUMENT, "out_color and background are required");
+  if (a->P > 0 && (a->radii == nullptr || a->opacities == nullptr))
+    return fail(OMNIGS_ERR_INVALID_ARGUMENT, "radii and opacities are required");
+  return OMNIGS_OK;
+}
+
+__global__ void begin_render_kernel(GeomHeader* hdr) {
+  atomicAnd(&hdr->status, ~kStatusCapacity);
+  for (int i = 0; i < kMaxSortPasses; ++i) hdr->sort_tile_counter[i] = 0;
+}
+
+__global__ void mark_visible_kernel(int P, const float* means3D, const float* vm, int camera_type,
+                                    uint8_t* present) {
+  const int idx = blockIdx.x * blockDim.x + threadIdx.x;
+  if (idx >= P) return;
+  if (camera_type == OMNIGS_CAMERA_LONLAT) {
+    present[idx] = 1;
+    return;
+  }
+  const float x = means3D[3 * idx], y = means3D[3 * idx + 1], z = means3D[3 * idx + 2];
+  const float pz = vm[2] * x + vm[6] * y + vm[10] * z + vm[14];
+  present[idx] = (pz <= 0.2f) ? 0 : 1;
+}
+
+}  // namespace
+
+void launch_mark_visible(int P, const float* means3D, const float* viewmatrix, int camera_type,
+                         bool* present, cudaStream_t s) {
+  if (P <= 0) return;
+  mark_visible_kernel<<<(P + 255) / 256, 256, 0, s>>>(P, means3D, viewmatrix, camera_type,
+                                                        reinterpret_cast<uint8_t*>(present));
+}
+
+}  // namespace omnigs
+
+using namespace omnigs;
+
+extern "C" {
+
+const char* omnigs_version(void) { return "omnigs_b200 0.1.0 (sm_100a)"; }
+
+const char* omnigs_last_error(void) { return g_last_error.c_str(); }
+
+size_t omnigs_lonlat_geom_bytes(int P) { return GeomLayout::make(P < 0 ? 0 : P).total; }
+
+size_t omnigs_lonlat_image_bytes(int W, int H) {
+  if (W <= 0 || H <= 0) return 0;
+  return ImageLayout::make(W, H).total;
+}
+
+size_t omnigs_lonlat_binning_bytes(int64_t capacity) {
+  return BinningLayout::make(capacity < 0 ? 0 : capacity).total;
+}
+
+int64_t omnigs_lonlat_binning_capacity(size_t binning_bytes) {
+  return BinningLayout::capacity_for(binning_bytes);
+}
+
+int omnigs_lonlat_preprocess(const OmnigsLonlatForwardArgs* a, void* geom, size_t geom_bytes,
+                             omnigs_stream_t stream) {
+  g_last_error.clear();
+  if (int rc = validate_forward(a)) return rc;
+  cudaStream_t s = reinterpret_cast<cudaStream_t>(stream);
+  const GeomLayout L = GeomLayout::make(a->P);
+  if (geom == nullptr || geom_bytes < L.total)
+    return fail(OMNIGS_ERR_BUFFER_TOO_SMALL, "geometry buffer smaller than omnigs_lonlat_geom_bytes(P)");
+  if (cudaMemsetAsync(geom, 0, L.zero_end, s) != cudaSuccess) return check_launch("memset geometry header");
+  if (a->P == 0) return OMNIGS_OK;
+  PreprocessParams p{};
+  p.P = a->P;
+  p.D = a->D;
+  p.M = a->M;
+  p.W = a->W;
+  p.H = a->H;
+  p.gx = tiles_x(a->W);
+  p.gy = tiles_y(a->H);
+  p.means3D = a->means3D;
+  p.scales = a->scales;
+  p.rotations = a->rotations;
+  p.opacities = a->opacities;
+  p.shs = a->shs;
+  p.colors_precomp = a->colors_precomp;
+  p.cov3D_precomp = a->cov3D_precomp;
+  p.scale_modifier = a->scale_modifier;
+  p.viewmatrix = a->viewmatrix;
+  p.campos = a->campos;
+  p.radii = a->radii;
+  p.splat = at<float4>(geom, L.splat);
+  p.color = at<float4>(geom, L.color);
+  p.depth = at<float>(geom, L.depth);
+  p.offsets = at<uint32_t>(geom, L.offsets);
+  p.grad_acc = at<float4>(geom, L.grad_acc);
+  p.scan_state = at<unsigned long long>(geom, L.scan_state);
+  p.hdr = at<GeomHeader>(geom, L.header);
+  staged(OMNIGS_STAGE_PREPROCESS, 1, s, [&] { launch_preprocess(p, s); });
+  return check_launch("preprocess");
+}
+
+int omnigs_lonlat_render(const OmnigsLonlatForwardArgs* a, void* geom, size_t geom_bytes,
+                         void* binning, size_t binning_bytes, void* image, size_t image_bytes,
+                         omnigs_stream_t stream) {
+  g_last_error.clear();
+  if (int rc = validate_forward(a)) return rc;
+  cudaStream_t s = reinterpret_cast<cudaStream_t>(stream);
+  const int64_t HW = (int64_t)a->W * a->H;
+  if (a->P == 0) {
+    // The reference returns its zero-initialised image when there are no Gaussians
+    // (src/rasterize_points.cu:84, 97).
+    if (cudaMemsetAsync(a->out_color, 0, sizeof(float) * 3 * HW, s) != cudaSuccess)
+      return check_launch("memset out_color");
+    return OMNIGS_OK;
+  }
+  const GeomLayout GL = GeomLayout::make(a->P);
+  const ImageLayout IL = ImageLayout::make(a->W, a->H);
+  if (geom == nullptr || geom_bytes < GL.total)
+    return fail(OMNIGS_ERR_BUFFER_TOO_SMALL, "geometry buffer smaller than omnigs_lonlat_geom_bytes(P)");
+  if (image == nullptr || image_bytes < IL.total)
+    return fail(OMNIGS_ERR_BUFFER_TOO_SMALL, "image buffer smaller than omnigs_lonlat_image_bytes(W, H)");
+  const int64_t capacity = BinningLayout::capacity_for(binning_bytes);
+  if (binning == nullptr || capacity < 0)
+    return fail(OMNIGS_ERR_BUFFER_TOO_SMALL, "binning buffer smaller than omnigs_lonlat_binning_bytes(0)");
+  const BinningLayout BL = BinningLayout::make(capacity);
+  const int gx = tiles_x(a->W), gy = tiles_y(a->H);
+  const int passes = sort_passes(a->W, a->H);
+  GeomHeader* hdr = at<GeomHeader>(geom, GL.header);
+  uint32_t* hist = at<uint32_t>(binning, BL.hist);
+  uint32_t* lookback = at<uint32_t>(binning, BL.lookback);
+  uint2* ranges = at<uint2>(image, IL.ranges);
+
+  staged(OMNIGS_STAGE_OTHER, 1, s, [&] { begin_render_kernel<<<1, 1, 0, s>>>(hdr); });
+  if (cudaMemsetAsync(hist, 0, sizeof(uint32_t) * kMaxSortPasses * kRadix, s) != cudaSuccess ||
+      cudaMemsetAsync(ranges, 0, sizeof(uint2) * (size_t)gx * gy, s) != cudaSuccess)
+    return check_launch("memset binning state");
+
+  DuplicateParams d{};
+  d.P = a->P;
+  d.gx = gx;
+  d.gy = gy;
+  d.passes = passes;
+  d.radii = a->radii;
+  d.splat = at<float4>(geom, GL.splat);
+  d.depth = at<float>(geom, GL.depth);
+  d.offsets = at<uint32_t>(geom, GL.offsets);
+  d.keys = at<uint64_t>(binning, BL.keys0);
+  d.vals = at<uint32_t>(binning, BL.vals0);
+  d.hist = hist;
+  d.lookback = lookback;
+  d.lookback_pass_stride = BinningLayout::sort_tiles(capacity) * kRadix;
+  d.capacity = capacity;
+  d.hdr = hdr;
+  staged(OMNIGS_STAGE_DUPLICATE, 1, s, [&] { launch_duplicate(d, s); });
+  if (int rc = check_launch("duplicate")) return rc;
+
+  uint64_t* keys[2] = {at<uint64_t>(binning, BL.keys0), at<uint64_t>(binning, BL.keys1)};
+  uint32_t* vals[2] = {at<uint32_t>(binning, BL.vals0), at<uint32_t>(binning, BL.vals1)};
+  for (int pass = 0; pass < passes; ++pass) {
+    SortPassParams sp{};
+    sp.keys_in = keys[pass & 1];
+    sp.vals_in = vals[pass & 1];
+    sp.keys_out = keys[(pass + 1) & 1];
+    sp.vals_out = vals[(pass + 1) & 1];
+    sp.hist = hist + pass * kRadix;
+    sp.lookback = lookback + pass * d.lookback_pass_stride;
+    sp.tile_counter = &hdr->sort_tile_counter[pass];
+    sp.shift = kRadixBits * pass;
+    sp.capacity = capacity;
+    sp.hdr = hdr;
+    staged(OMNIGS_STAGE_SORT, 1, s, [&] { launch_sort_pass(sp, s); });
+    if (int rc = check_launch("sort pass")) return rc;
+  }
+  const int fin = passes & 1;
+
+  RangesParams rp{};
+  rp.keys = keys[fin];
+  rp.ranges = ranges;
+  rp.num_tiles = (uint32_t)gx * (uint32_t)gy;
+  rp.capacity = capacity;
+  rp.hdr = hdr;
+  staged(OMNIGS_STAGE_RANGES, 1, s, [&] { launch_ranges(rp, s); });
+  if (int rc = check_launch("ranges")) return rc;
+
+  RenderParams r{};
+  r.P = a->P;
+  r.W = a->W;
+  r.H = a->H;
+  r.gx = gx;
+  r.gy = gy;
+  r.ranges = ranges;
+  r.point_list = vals[fin];
+  r.capacity = capacity;
+  r.splat = at<float4>(geom, GL.splat);
+  r.color = at<float4>(geom, GL.color);
+  r.bg = a->background;
+  r.out_color = a->out_color;
+  r.final_T = at<float>(image, IL.final_T);
+  r.n_contrib = at<uint32_t>(image, IL.n_contrib);
+  staged(OMNIGS_STAGE_RENDER_FORWARD, 1, s, [&] { launch_render_forward(r, s); });
+  return check_launch("render forward");
+}
+
+int omnigs_lonlat_forward(const OmnigsLonlatForwardArgs* a, void* geom, size_t geom_bytes,
+                          void* binning, size_t binning_bytes, void* image, size_t image_bytes,
+                          omnigs_stream_t stream) {
+  if (int rc = omnigs_lonlat_preprocess(a, geom, geom_bytes, stream)) return rc;
+  return omnigs_lonlat_render(a, geom, geom_bytes, binning, binning_bytes, image, image_bytes, stream);
+}
+
+int omnigs_lonlat_read_status(const void* geom, int* num_rendered, uint32_t* status,
+                              omnigs_stream_t stream) {
+  g_last_error.clear();
+  if (geom == nullptr) return fail(OMNIGS_ERR_INVALID_ARGUMENT, "geom is NULL");
+  GeomHeader h;
+  cudaStream_t s = reinterpret_cast<cudaStream_t>(stream);
+  if (cudaMemcpyAsync(&h, geom, sizeof(h), cudaMemcpyDeviceToHost, s) != cudaSuccess)
+    return check_launch("read status");
+  if (cudaStreamSynchronize(s) != cudaSuccess) return check_launch("synchronize");
+  if (num_rendered) *num_rendered = (int)(h.num_rendered64 > 0x7fffffffull ? 0x7fffffff : h.num_rendered64);
+  if (status) *status = h.status;
+  return OMNIGS_OK;
+}
+
+int omnigs_lonlat_backward(const OmnigsLonlatBackwardArgs* a, void* geom, size_t geom_bytes,
+                           const void* binning, size_t binning_bytes, const void* image,
+                           size_t image_bytes, omnigs_stream_t stream) {
+  g_last_error.clear();
+  if (a == nullptr) return fail(OMNIGS_ERR_INVALID_ARGUMENT, "args is NULL");
+  if (int rc = validate_common(a->P, a->D, a->M, a->W, a->H, a->shs, a->colors_precomp, a->scales,
+                               a->rotations, a->cov3D_precomp, a->means3D, a->viewmatrix, a->campos))
+    return rc;
+  if (a->P == 0) return OMNIGS_OK;
+  if (a->radii == nullptr || a->dL_dout_color == nullptr || a->background == nullptr ||
+      a->dL_dmeans2D == nullptr || a->dL_dcolors == nullptr || a->dL_dopacity == nullptr ||
+      a->dL_dmeans3D == nullptr || a->dL_dcov3D == nullptr || a->dL_dscales == nullptr ||
+      a->dL_drotations == nullptr || (a->M > 0 && a->shs != nullptr && a->dL_dsh == nullptr))
+    return fail(OMNIGS_ERR_INVALID_ARGUMENT, "a required backward input or output is NULL");
+  cudaStream_t s = reinterpret_cast<cudaStream_t>(stream);
+  const GeomLayout GL = GeomLayout::make(a->P);
+  const ImageLayout IL = ImageLayout::make(a->W, a->H);
+  if (geom == nullptr || geom_bytes < GL.total)
+    return fail(OMNIGS_ERR_BUFFER_TOO_SMALL, "geometry buffer smaller than omnigs_lonlat_geom_bytes(P)");
+  if (image == nullptr || image_bytes < IL.total)
+    return fail(OMNIGS_ERR_BUFFER_TOO_SMALL, "image buffer smaller than omnigs_lonlat_image_bytes(W, H)");
+  const int64_t capacity = BinningLayout::capacity_for(binning_bytes);
+  if (binning == nullptr || capacity < 0)
+    return fail(OMNIGS_ERR_BUFFER_TOO_SMALL, "binning buffer smaller than omnigs_lonlat_binning_bytes(0)");
+  if (a->R > capacity) return fail(OMNIGS_ERR_CAPACITY, "R exceeds the binning buffer's capacity");
+  const BinningLayout BL = BinningLayout::make(capacity);
+  const int gx = tiles_x(a->W), gy = tiles_y(a->H);
+  const int fin = sort_passes(a->W, a->H) & 1;
+
+  RenderParams r{};
+  r.P = a->P;
+  r.W = a->W;
+  r.H = a->H;
+  r.gx = gx;
+  r.gy = gy;
+  r.ranges = at<uint2>(image, IL.ranges);
+  r.point_list = at<uint32_t>(binning, fin ? BL.vals1 : BL.vals0);
+  r.capacity = capacity;
+  r.splat = at<float4>(geom, GL.splat);
+  r.color = at<float4>(geom, GL.color);
+  r.bg = a->background;
+  r.final_T = const_cast<float*>(at<float>(image, IL.final_T));
+  r.n_contrib = const_cast<uint32_t*>(at<uint32_t>(image, IL.n_contrib));
+  r.dL_dpix = a->dL_dout_color;
+  r.grad_acc = at<float>(geom, GL.grad_acc);
+  staged(OMNIGS_STAGE_RENDER_BACKWARD, 1, s, [&] { launch_render_backward(r, s); });
+  if (int rc = check_launch("render backward")) return rc;
+
+  PreprocessBackwardParams b{};
+  b.P = a->P;
+  b.D = a->D;
+  b.M = a->M;
+  b.W = a->W;
+  b.H = a->H;
+  b.means3D = a->means3D;
+  b.radii = a->radii;
+  b.shs = a->shs;
+  b.color = at<float4>(geom, GL.color);
+  b.scales = a->scales;
+  b.rotations = a->rotations;
+  b.cov3D_precomp = a->cov3D_precomp;
+  b.scale_modifier = a->scale_modifier;
+  b.viewmatrix = a->viewmatrix;
+  b.campos = a->campos;
+  b.grad_acc = at<float4>(geom, GL.grad_acc);
+  b.dL_dmeans2D = a->dL_dmeans2D;
+  b.dL_dconic = a->dL_dconic;
+  b.dL_dopacity = a->dL_dopacity;
+  b.dL_dcolors = a->dL_dcolors;
+  b.dL_dmeans3D = a->dL_dmeans3D;
+  b.dL_dcov3D = a->dL_dcov3D;
+  b.dL_dsh = a->dL_dsh;
+  b.dL_dscales = a->dL_dscales;
+  b.dL_drotations = a->dL_drotations;
+  staged(OMNIGS_STAGE_PREPROCESS_BACKWARD, 1, s, [&] { launch_preprocess_backward(b, s); });
+  return check_launch("preprocess backward");
+}
+
+int omnigs_mark_visible(int P, const float* means3D, const float* viewmatrix, int camera_type,
+                        uint8_t* present, omnigs_stream_t stream) {
+  g_last_error.clear();
+  if (P < 0) return fail(OMNIGS_ERR_INVALID_ARGUMENT, "P must be >= 0");
+  if (camera_type != OMNIGS_CAMERA_LONLAT && camera_type != OMNIGS_CAMERA_PINHOLE)
+    return fail(OMNIGS_ERR_INVALID_ARGUMENT, "[CudaRasterizer]Invalid camera_type");
+  if (P == 0) return OMNIGS_OK;
+  if (present == nullptr || (camera_type == OMNIGS_CAMERA_PINHOLE && (means3D == nullptr || viewmatrix == nullptr)))
+    return fail(OMNIGS_ERR_INVALID_ARGUMENT, "present, means3D and viewmatrix are required");
+  cudaStream_t s = reinterpret_cast<cudaStream_t>(stream);
+  staged(OMNIGS_STAGE_OTHER, 1, s, [&] {
+    launch_mark_visible(P, means3D, viewmatrix, camera_type, reinterpret_cast<bool*>(present), s);
+  });
+  return check_launch("mark visible");
+}
+
+int omnigs_timing_enable(int enable) {
+  std::lock_guard<std::mutex> lock(g_timing_mu);
+  g_timing.store(enable != 0);
+  return OMNIGS_OK;
+}
+
+int omnigs_timing_read(OmnigsStageTimes* out) {
+  g_last_error.clear();
+  if (out == nullptr) return fail(OMNIGS_ERR_INVALID_ARGUMENT, "out is NULL");
+  std::memset(out, 0, sizeof(*out));
+  std::lock_guard<std::mutex> lock(g_timing_mu);
+  int rc = OMNIGS_OK;
+  for (const TimedLaunch& t : g_timed) {
+    float ms = 0.f;
+    if (cudaEventSynchronize(t.stop) != cudaSuccess || cudaEventElapsedTime(&ms, t.start, t.stop) != cudaSuccess)
+      rc = check_launch("timing read");
+    out->ms[t.stage] += ms;
+    out->launches[t.stage] += (uint64_t)t.kernels;
+    g_event_pool.push_back(t.start);
+    g_event_pool.push_back(t.stop);
+  }
+  g_timed.clear();
+  return rc;
+}
+
+uint64_t omnigs_kernel_launches(void) { return g_launches.load(); }
+
+int omnigs_lonlat_geom_view(const void* geom, int P, OmnigsLonlatGeomView* out) {
+  if (geom == nullptr || out == nullptr || P < 0) return fail(OMNIGS_ERR_INVALID_ARGUMENT, "bad view arguments");
+  const GeomLayout L = GeomLayout::make(P);
+  out->splat = at<float>(geom, L.splat);
+  out->color = at<float>(geom, L.color);
+  out->depth = at<float>(geom, L.depth);
+  out->offsets = at<uint32_t>(geom, L.offsets);
+  return OMNIGS_OK;
+}
+
+int omnigs_lonlat_binning_view(const void* binning, size_t binning_bytes, int W, int H,
+                               OmnigsLonlatBinningView* out) {
+  if (binning == nullptr || out == nullptr || W <= 0 || H <= 0)
+    return fail(OMNIGS_ERR_INVALID_ARGUMENT, "bad view arguments");
+  const int64_t capacity = BinningLayout::capacity_for(binning_bytes);
+  if (capacity < 0) return fail(OMNIGS_ERR_BUFFER_TOO_SMALL, "binning buffer too small");
+  const BinningLayout L = BinningLayout::make(capacity);
+  const int fin = sort_passes(W, H) & 1;
+  out->keys = at<uint64_t>(binning, fin ? L.keys1 : L.keys0);
+  out->point_list = at<uint32_t>(binning, fin ? L.vals1 : L.vals0);
+  return OMNIGS_OK;
+}
+
+int omnigs_lonlat_image_view(const void* image, int W, int H, OmnigsLonlatImageView* out) {
+  if (image == nullptr || out == nullptr || W <= 0 || H <= 0)
+    return fail(OMNIGS_ERR_INVALID_ARGUMENT, "bad view arguments");
+  const ImageLayout L = ImageLayout::make(W, H);
+  out->final_T = at<float>(image, L.final_T);
+  out->n_contrib = at<uint32_t>(image, L.n_contrib);
+  out->ranges = at<uint32_t>(image, L.ranges);
+  return OMNIGS_OK;
+}
+
+}  // extern "C"
