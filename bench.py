@@ -53,6 +53,10 @@ def parse():
     ap.add_argument("--impl", default="omnigs", choices=["omnigs", "reference"])
     ap.add_argument("--no-cpu-baseline", action="store_true")
     ap.add_argument("--no-e2e", action="store_true")
+    # smaller cases for profiling captures only; bench lines use the defaults
+    ap.add_argument("--gaussians", type=int, default=P_GAUSS)
+    ap.add_argument("--width", type=int, default=WIDTH)
+    ap.add_argument("--height", type=int, default=HEIGHT)
     return ap.parse_args()
 
 
@@ -215,13 +219,13 @@ def run_omnigs(args, rank, world, local_rank):
 
     dev = torch.device("cuda", local_rank)
     torch.cuda.set_device(dev)
-    g = scenes.make_gaussians(P_GAUSS, seed=0)
-    view = scenes.identity_view(WIDTH, HEIGHT)
-    dpix_np = scenes.upstream_grad(WIDTH, HEIGHT, seed=2 + rank)
+    g = scenes.make_gaussians(args.gaussians, seed=0)
+    view = scenes.identity_view(args.width, args.height)
+    dpix_np = scenes.upstream_grad(args.width, args.height, seed=2 + rank)
     gt = lonlat.GaussianTensors.from_numpy(g, dev)
     cam = lonlat.Camera.from_view(view, dev)
     dpix = torch.from_numpy(dpix_np).to(dev)
-    P, W, H = g.P, WIDTH, HEIGHT
+    P, W, H = g.P, args.width, args.height
 
     # sizing pass (untimed): exact instance count, then a fixed capacity for the timed steps
     _, radii0, n0, _ = lonlat.rasterize(gt, cam)
@@ -372,11 +376,13 @@ def run_omnigs(args, rank, world, local_rank):
         cpu = cpu_baseline(g, view, dpix_np)
 
     if rank == 0:
+        workload = WORKLOAD if (P, W, H) == (P_GAUSS, WIDTH, HEIGHT) else \
+            f"profiling case: {P} Gaussians, {W}x{H} (not a bench line)"
         line = {"metric": METRIC, "value": round(value, 3), "unit": UNIT, "n_gpus": world,
                 "steps": args.steps, "warmup": args.warmup, "ms_per_step": round(ms_per_step, 4),
                 "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "f32",
                 "data": "synthetic (seeded generators of the reference's config shapes)",
-                "config": {"workload": WORKLOAD, "gaussians": P, "width": W, "height": H,
+                "config": {"workload": workload, "gaussians": P, "width": W, "height": H,
                            "num_rendered": n0, "visible": V, "parallelism": f"dp{world} (views)",
                            "l2": "inputs larger than L2 (SH alone 192 MB > 126 MB), no flush"},
                 "gpu_launches": int(launches), "clocks": clocks.summary(), "roofline": roofline,

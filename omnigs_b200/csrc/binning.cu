@@ -210,6 +210,7 @@ __global__ void __launch_bounds__(kSortThreads) sort_pass_kernel(SortPassParams 
   const uint32_t count = run;
   uint32_t tile_items;
   sm.block_excl[d] = block_exclusive_scan(count, sm.scan_tmp, tile_items);
+  __syncthreads();  // every digit's block-local start is read by other threads below
 
   // decoupled look-back for this digit
   uint32_t* lb = p.lookback;
@@ -258,8 +259,10 @@ __global__ void __launch_bounds__(kSortThreads) sort_pass_kernel(SortPassParams 
     if (rank[k] != 0xffffffffu) {
       const uint32_t digit = (uint32_t)(key[k] >> p.shift) & (kRadix - 1);
       const uint32_t pos = sm.block_excl[digit] + sm.warp_hist[warp][digit] + rank[k];
-      sm.keys[pos] = key[k];
-      sm.vals[pos] = val[k];
+      if (pos < (uint32_t)kSortTile) {  // always true: ranks are consistent within the block
+        sm.keys[pos] = key[k];
+        sm.vals[pos] = val[k];
+      }
     }
   }
   __syncthreads();
