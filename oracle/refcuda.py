@@ -79,26 +79,32 @@ class ReferenceRasterizer:
     def __del__(self):
         self.close()
 
-    def forward(self, g, cam, D=3, scale_modifier=1.0):
-        """Returns (image [3,H,W], radii [P], num_rendered).  ``g``/``cam`` as in omnigs_b200.lonlat."""
-        torch.cuda.synchronize()
-        out = torch.zeros(3, cam.height, cam.width, dtype=torch.float32, device="cuda")
-        radii = torch.zeros(g.P, dtype=torch.int32, device="cuda")
+    def forward(self, g, cam, D=3, scale_modifier=1.0, sync=True, out=None, radii=None):
+        """Returns (image [3,H,W], radii [P], num_rendered).  ``g``/``cam`` as in omnigs_b200.lonlat.
+        ``sync=False`` skips this wrapper's own device synchronisation (for timing)."""
+        if sync:
+            torch.cuda.synchronize()
+        out = torch.zeros(3, cam.height, cam.width, dtype=torch.float32, device="cuda") if out is None else out
+        radii = torch.zeros(g.P, dtype=torch.int32, device="cuda") if radii is None else radii
         R = lib().ref_forward(self.h, g.P, D, g.M, _p(cam.background), cam.width, cam.height,
                               _p(g.means3D), _p(g.shs), _p(g.colors_precomp), _p(g.opacities),
                               _p(g.scales), scale_modifier, _p(g.rotations), _p(g.cov3D_precomp),
                               _p(cam.viewmatrix), _p(cam.campos), _p(out), _p(radii))
-        torch.cuda.synchronize()
+        if sync:
+            torch.cuda.synchronize()
         self.P, self.W, self.H = g.P, cam.width, cam.height
         return out, radii, int(R)
 
-    def backward(self, g, cam, radii, dL_dpix, D=3, scale_modifier=1.0):
+    def backward(self, g, cam, radii, dL_dpix, D=3, scale_modifier=1.0, sync=True):
+        """Zero-initialised gradient outputs as the reference's LibTorch layer allocates them
+        (src/rasterize_points.cu:200-208), then the reference backward."""
         P, M = g.P, g.M
         z = lambda *s: torch.zeros(*s, dtype=torch.float32, device="cuda")  # noqa: E731
         out = dict(dL_dmeans2D=z(P, 3), dL_dconic=z(P, 2, 2), dL_dopacity=z(P, 1),
                    dL_dcolors=z(P, 3), dL_dmeans3D=z(P, 3), dL_dcov3D=z(P, 6), dL_dsh=z(P, M, 3),
                    dL_dscales=z(P, 3), dL_drotations=z(P, 4))
-        torch.cuda.synchronize()
+        if sync:
+            torch.cuda.synchronize()
         lib().ref_backward(self.h, D, M, _p(cam.background), _p(g.means3D), _p(g.shs),
                            _p(g.colors_precomp), _p(g.scales), scale_modifier, _p(g.rotations),
                            _p(g.cov3D_precomp), _p(cam.viewmatrix), _p(cam.campos), _p(radii),
@@ -106,7 +112,8 @@ class ReferenceRasterizer:
                            _p(out["dL_dopacity"]), _p(out["dL_dcolors"]), _p(out["dL_dmeans3D"]),
                            _p(out["dL_dcov3D"]), _p(out["dL_dsh"]), _p(out["dL_dscales"]),
                            _p(out["dL_drotations"]))
-        torch.cuda.synchronize()
+        if sync:
+            torch.cuda.synchronize()
         return out
 
     def state(self) -> dict:
