@@ -138,6 +138,19 @@ int omnigs_lonlat_forward(const OmnigsLonlatForwardArgs* args, void* geom, size_
                           void* binning, size_t binning_bytes, void* image, size_t image_bytes,
                           omnigs_stream_t stream);
 
+/* omnigs_lonlat_forward for callers that cannot allocate device memory (a plugin inside a host
+ * application that owns all device memory, or a fixed-budget real-time loop that must not call
+ * cudaMalloc).  This entry point has no counterpart in the reference.  The geometry, image and
+ * binning state live in a 16 MiB __device__ array inside this library (held by every GPU that
+ * loads it until exit), so the caller passes only inputs and outputs.  Limits: P <= 32768,
+ * W * H <= 262144 and the instances must fit the rest of the array (OMNIGS_ERR_CAPACITY
+ * otherwise).  It allocates no device memory; it waits for `stream` at the end to read the status
+ * and returns num_rendered.  The first call on a device looks up the array's device address
+ * (cudaGetSymbolAddress); make that first call before any stream capture.  All calls share the
+ * array: calls that overlap on the GPU race and must not be issued. */
+int omnigs_lonlat_forward_noalloc(const OmnigsLonlatForwardArgs* args, int* num_rendered,
+                                  omnigs_stream_t stream);
+
 /* Waits for `stream` and copies num_rendered and the status word to the host.  The one call that
  * synchronises; the reference's forward returns num_rendered by value (rasterizer.h:104). */
 int omnigs_lonlat_read_status(const void* geom, int* num_rendered, uint32_t* status,

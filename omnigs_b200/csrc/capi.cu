@@ -138,6 +138,8 @@ __global__ void mark_visible_kernel(int P, const float* means3D, const float* vm
 
 }  // namespace
 
+void set_last_error(const char* msg) { g_last_error = msg; }
+
 void launch_mark_visible(int P, const float* means3D, const float* viewmatrix, int camera_type,
                          bool* present, cudaStream_t s) {
   if (P <= 0) return;

@@ -113,6 +113,9 @@ void launch_ranges(const RangesParams& p, cudaStream_t s);
 void launch_render_forward(const RenderParams& p, cudaStream_t s);
 void launch_render_backward(const RenderParams& p, cudaStream_t s);
 void launch_preprocess_backward(const PreprocessBackwardParams& p, cudaStream_t s);
+// Sets the message returned by omnigs_last_error() on this host thread.
+void set_last_error(const char* msg);
+
 void launch_mark_visible(int P, const float* means3D, const float* viewmatrix, int camera_type,
                          bool* present, cudaStream_t s);
 
