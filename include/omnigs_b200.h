@@ -195,14 +195,17 @@ uint64_t omnigs_kernel_launches(void);
 /* Read-only views into the private buffers, for inspection and parity testing.  Pointers are
  * device pointers inside the given buffers. */
 typedef struct OmnigsLonlatGeomView {
-  const float* splat;       /* [P][8]: x, y, conic a, conic b, conic c, opacity, cull hx, cull hy */
-  const float* color;       /* [P][4]: r, g, b, clamp bits (as uint32) */
-  const float* depth;       /* [P] radial distance r */
-  const uint32_t* offsets;  /* [P] inclusive scan of tiles_touched */
+  const float* splat;          /* [P][8]: x, y, conic a, conic b, conic c, opacity, cull hx, cull hy */
+  const float* color;          /* [P][4]: r, g, b, clamp bits (as uint32) */
+  const float* depth;          /* [P] radial distance r (+inf where culled) */
+  const uint32_t* tiles_touched; /* [P] */
+  const uint32_t* depth_order; /* [P] Gaussian indices sorted by (depth bits, index) */
 } OmnigsLonlatGeomView;
+/* The sorted instance list: instance i covers tile tile_ids[i] and Gaussian point_list[i]; the
+ * reference's 64-bit key of instance i is tile_ids[i] << 32 | float_bits(depth[point_list[i]]). */
 typedef struct OmnigsLonlatBinningView {
-  const uint64_t* keys;     /* [num_rendered] sorted tile|depth keys */
-  const uint32_t* point_list; /* [num_rendered] sorted Gaussian indices */
+  const uint32_t* tile_ids;    /* [num_rendered] sorted tile ids */
+  const uint32_t* point_list;  /* [num_rendered] sorted Gaussian indices */
 } OmnigsLonlatBinningView;
 typedef struct OmnigsLonlatImageView {
   const float* final_T;     /* [H*W] */

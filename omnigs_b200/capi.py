@@ -55,11 +55,12 @@ class StageTimes(ctypes.Structure):
 
 
 class GeomView(ctypes.Structure):
-    _fields_ = [("splat", _vp), ("color", _vp), ("depth", _vp), ("offsets", _vp)]
+    _fields_ = [("splat", _vp), ("color", _vp), ("depth", _vp), ("tiles_touched", _vp),
+                ("depth_order", _vp)]
 
 
 class BinningView(ctypes.Structure):
-    _fields_ = [("keys", _vp), ("point_list", _vp)]
+    _fields_ = [("tile_ids", _vp), ("point_list", _vp)]
 
 
 class ImageView(ctypes.Structure):

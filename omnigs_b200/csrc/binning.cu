@@ -1,21 +1,21 @@
-// Binning: tile/depth key duplication, a stable onesweep LSD radix sort, and tile ranges.
+// Binning: the reference's sorted instance list and tile ranges (rasterizer_impl.cu:94-167,
+// 622-679) from a depth sort of the Gaussians plus a tile sort of the instances.
 //
-// Reference: duplicateWithKeys (rasterizer_impl.cu:94-140), cub::DeviceRadixSort::SortPairs over
-// key bits [0, 32 + getHigherMsb(tiles)) (:651-661), identifyTileRanges (:145-167).
-//
-// * duplicate: each warp owns 32 consecutive Gaussians, whose instances occupy one contiguous
-//   output span (their offsets are consecutive).  The warp walks that span 32 instances at a time,
-//   finds each instance's owner with a 5-step shuffle search over the lanes' start offsets, and
-//   writes keys/values fully coalesced, so a splat covering hundreds of tiles no longer serialises
-//   one thread.  The same pass accumulates the 8-bit digit histograms of every sort pass.
-// * sort: one kernel per 8-bit digit.  A block ranks a 4096-key tile in shared memory (warp
-//   multi-split with match.any, which keeps equal digits in input order, so the sort is stable),
-//   publishes its per-digit counts, resolves its global digit offsets by decoupled look-back
-//   (blocks take tiles in launch order from an atomic counter) and scatters.  A stable LSD sort
-//   over the same bit range yields exactly cub's order: by key, ties in unsorted order.
-// * ranges: per-tile [start, end) over the sorted keys.
-// Instance counts live only on the device; every kernel reads num_rendered from the geometry
-// header and does nothing if it exceeds the binning capacity.
+// The reference emits one (tile << 32 | depth_bits) key per (Gaussian, tile) pair in Gaussian
+// order and sorts them with a stable LSD radix sort over bits [0, 32 + getHigherMsb(tiles)).  The
+// result is fully determined: instances ordered by tile, then by depth bits, then -- a Gaussian
+// appears at most once per tile and the list starts in Gaussian order -- by Gaussian index.  The
+// same order is produced here with far fewer passes over the instances:
+//  1. depth sort: a stable LSD radix sort (4 onesweep passes of 8 bits) of the P Gaussians by the
+//     bits of their depth, i.e. the order (depth bits, index);
+//  2. duplicate: instances are emitted walking the Gaussians in that order, each block scanning
+//     its Gaussians' tile counts and joining a decoupled look-back for its output offset;
+//  3. tile sort: a stable LSD radix sort (2 onesweep passes) of the instances by tile id only.
+// Stability makes (1)+(3) equal to the reference's single sort: instance passes drop from six
+// over 12-byte items to two over 8-byte items; the four depth passes run over P, not R, items.
+//  4. ranges: per-tile [start, end) over the sorted tile ids.
+// Counts live on the device: every kernel reads num_rendered from the geometry header and does no
+// work if it exceeds the binning capacity.  Waits on other blocks are bounded.
 #include <algorithm>
 
 #include "device_util.cuh"
@@ -28,94 +28,49 @@ namespace {
 constexpr uint32_t kLbAggregate = 1u << 30;
 constexpr uint32_t kLbPrefix = 2u << 30;
 constexpr uint32_t kLbValue = (1u << 30) - 1;
-constexpr int kDupThreads = 256;
+constexpr unsigned long long kScanAggregate = 1ull << 62;
+constexpr unsigned long long kScanPrefix = 2ull << 62;
+constexpr unsigned long long kScanValue = (1ull << 62) - 1;
 constexpr int kLookbackBatch = 8;
 
-__device__ __forceinline__ bool capacity_ok(const GeomHeader* hdr, int64_t capacity) {
-  const unsigned long long R = hdr->num_rendered64;
-  return (hdr->status & kStatusOverflow) == 0 && R <= (unsigned long long)capacity;
+__device__ __forceinline__ bool instances_fit(const GeomHeader* hdr, int64_t capacity) {
+  return (hdr->status & kStatusOverflow) == 0 && hdr->num_rendered64 <= (unsigned long long)capacity;
 }
 
-__global__ void __launch_bounds__(kDupThreads) duplicate_kernel(DuplicateParams p) {
-  __shared__ uint32_t s_hist[kMaxSortPasses][kRadix];
-  for (int i = threadIdx.x; i < kMaxSortPasses * kRadix; i += kDupThreads) (&s_hist[0][0])[i] = 0;
+// Element count of a sort/histogram: a host value, or the device num_rendered (0 if it does not
+// fit the capacity, in which case the duplicate pass has flagged the overflow).
+__device__ __forceinline__ uint32_t item_count(const GeomHeader* count_hdr, uint32_t n_host, int64_t capacity) {
+  if (count_hdr == nullptr) return n_host;
+  return instances_fit(count_hdr, capacity) ? count_hdr->num_rendered : 0u;
+}
+
+// ---------------------------------------------------------------- digit histograms ------------
+__global__ void __launch_bounds__(256) histogram_kernel(HistParams p) {
+  __shared__ uint32_t s_hist[kDepthPasses][kRadix];
+  for (int i = threadIdx.x; i < kDepthPasses * kRadix; i += blockDim.x) (&s_hist[0][0])[i] = 0;
   __syncthreads();
-  if (!capacity_ok(p.hdr, p.capacity)) {
-    if (blockIdx.x == 0 && threadIdx.x == 0) atomicOr(&p.hdr->status, kStatusCapacity);
-    return;
-  }
-  const uint32_t R = p.hdr->num_rendered;
-  // clear the sort look-back words of the tiles this sort will use
-  {
-    const int64_t ntiles = (R + kSortTile - 1) / kSortTile;
-    const int64_t n = ntiles * kRadix;
-    for (int pass = 0; pass < p.passes; ++pass)
-      for (int64_t i = blockIdx.x * (int64_t)kDupThreads + threadIdx.x; i < n;
-           i += (int64_t)gridDim.x * kDupThreads)
-        p.lookback[pass * p.lookback_pass_stride + i] = 0;
-  }
+  const uint32_t n = item_count(p.count_hdr, p.n_host, p.capacity);
   const int lane = threadIdx.x & 31;
-  const int warps_total = gridDim.x * (kDupThreads / 32);
-  for (int base = (blockIdx.x * (kDupThreads / 32) + (threadIdx.x >> 5)) * 32; base < p.P;
-       base += warps_total * 32) {
-    const int g = base + lane;
-    uint32_t start = R, count = 0, dbits = 0;
-    int rminx = 0, rminy = 0, width = 1;
-    if (g < p.P) {
-      start = (g == 0) ? 0u : p.offsets[g - 1];
-      const int radius = p.radii[g];
-      if (radius > 0) {
-        const float4 a = p.splat[2 * g];
-        int2 rmin, rmax;
-        tile_rect(make_float2(a.x, a.y), radius, p.gx, p.gy, rmin, rmax);
-        rminx = rmin.x;
-        rminy = rmin.y;
-        width = rmax.x - rmin.x;
-        count = p.offsets[g] - start;
-        dbits = __float_as_uint(p.depth[g]);
-      }
-    }
-    const uint32_t w_begin = __shfl_sync(kFullMask, start, 0);
-    const uint32_t w_end = __shfl_sync(kFullMask, start + count, 31);
-    for (uint32_t o0 = w_begin; o0 < w_end; o0 += 32) {
-      const uint32_t o = o0 + lane;
-      const bool valid = o < w_end;
-      int pos = 0;
-#pragma unroll
-      for (int step = 16; step > 0; step >>= 1) {
-        const uint32_t s = __shfl_sync(kFullMask, start, pos + step);
-        if (s <= o) pos += step;
-      }
-      const uint32_t o_start = __shfl_sync(kFullMask, start, pos);
-      const int o_rminx = __shfl_sync(kFullMask, rminx, pos);
-      const int o_rminy = __shfl_sync(kFullMask, rminy, pos);
-      const int o_width = __shfl_sync(kFullMask, width, pos);
-      const uint32_t o_dbits = __shfl_sync(kFullMask, dbits, pos);
-      uint64_t key = 0;
-      if (valid) {
-        const uint32_t local = o - o_start;
-        const uint32_t ty = (uint32_t)o_rminy + local / (uint32_t)o_width;
-        const uint32_t tx = (uint32_t)o_rminx + local % (uint32_t)o_width;
-        key = ((uint64_t)(ty * (uint32_t)p.gx + tx) << 32) | o_dbits;
-        p.keys[o] = key;
-        p.vals[o] = (uint32_t)(base + pos);
-      }
-      for (int pass = 0; pass < p.passes; ++pass) {
-        const uint32_t digit = (uint32_t)(key >> (kRadixBits * pass)) & (kRadix - 1);
-        const uint32_t tag = valid ? digit : (0x10000u + lane);
-        const unsigned peers = __match_any_sync(kFullMask, tag);
-        if (valid && lane == __ffs(peers) - 1) atomicAdd(&s_hist[pass][digit], (uint32_t)__popc(peers));
-      }
+  const uint32_t stride = gridDim.x * blockDim.x;
+  // whole warps iterate together so that match.any sees all 32 lanes
+  for (uint32_t base = blockIdx.x * blockDim.x + (threadIdx.x & ~31u); base < n; base += stride) {
+    const uint32_t i = base + lane;
+    const bool valid = i < n;
+    const uint32_t key = valid ? p.keys[i] : 0u;
+    for (int q = 0; q < p.passes; ++q) {
+      const uint32_t digit = (key >> p.shift[q]) & p.mask[q];
+      const unsigned peers = __match_any_sync(kFullMask, valid ? digit : (0x10000u | lane));
+      if (valid && lane == __ffs(peers) - 1) atomicAdd(&s_hist[q][digit], (uint32_t)__popc(peers));
     }
   }
   __syncthreads();
-  for (int i = threadIdx.x; i < p.passes * kRadix; i += kDupThreads) {
+  for (int i = threadIdx.x; i < p.passes * kRadix; i += blockDim.x) {
     const uint32_t v = (&s_hist[0][0])[i];
     if (v) atomicAdd(&p.hist[i], v);
   }
 }
 
-// Dynamic shared memory of one sort tile.
+// ---------------------------------------------------------------- onesweep pass ---------------
 struct SortSmem {
   uint32_t warp_hist[kSortThreads / 32][kRadix];
   uint32_t block_excl[kRadix];
@@ -123,7 +78,7 @@ struct SortSmem {
   uint32_t scan_tmp[kSortThreads / 32];
   uint32_t tile;
   uint32_t pad[3];
-  uint64_t keys[kSortTile];
+  uint32_t keys[kSortTile];
   uint32_t vals[kSortTile];
 };
 
@@ -154,12 +109,15 @@ __device__ __forceinline__ uint32_t block_exclusive_scan(uint32_t v, uint32_t* s
   return r;
 }
 
-__global__ void __launch_bounds__(kSortThreads) sort_pass_kernel(SortPassParams p) {
-  extern __shared__ __align__(16) unsigned char smem_raw[];
-  SortSmem& sm = *reinterpret_cast<SortSmem*>(smem_raw);
-  if (!capacity_ok(p.hdr, p.capacity)) return;
-  const uint32_t R = p.hdr->num_rendered;
-  const uint32_t ntiles = (R + kSortTile - 1) / kSortTile;
+// One stable LSD pass over (u32 key, u32 value) pairs on the digit (key >> shift) & mask.  A block
+// ranks a 4096-item tile in shared memory (warp multi-split with match.any: equal digits keep
+// their input order), publishes its per-digit counts, resolves its global digit offsets by
+// decoupled look-back (tiles are taken in launch order from an atomic counter, so a block only
+// waits on blocks that are already running) and writes runs of equal digits coalesced.
+__global__ void __launch_bounds__(kSortThreads, 3) onesweep_kernel(OnesweepParams p) {
+  __shared__ SortSmem sm;
+  const uint32_t n = item_count(p.count_hdr, p.n_host, p.capacity);
+  const uint32_t ntiles = (n + kSortTile - 1) / kSortTile;
   if (threadIdx.x == 0) sm.tile = atomicAdd(p.tile_counter, 1u);
   for (int i = threadIdx.x; i < (kSortThreads / 32) * kRadix; i += kSortThreads) (&sm.warp_hist[0][0])[i] = 0;
   __syncthreads();
@@ -167,25 +125,32 @@ __global__ void __launch_bounds__(kSortThreads) sort_pass_kernel(SortPassParams 
   if (tile >= ntiles) return;
   const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
   const unsigned lt_mask = (1u << lane) - 1u;
+  const uint32_t mask = p.mask;
+  const int shift = p.shift;
 
+  // load the whole tile first (independent loads in flight), then rank
+  uint32_t key[kSortItems], val[kSortItems];
+  const uint32_t tile_base = tile * kSortTile + warp * (kSortItems * 32) + lane;
+#pragma unroll
+  for (int k = 0; k < kSortItems; ++k) {
+    const uint32_t idx = tile_base + k * 32;
+    key[k] = idx < n ? p.keys_in[idx] : 0xffffffffu;
+  }
+#pragma unroll
+  for (int k = 0; k < kSortItems; ++k) {
+    const uint32_t idx = tile_base + k * 32;
+    val[k] = idx < n ? (p.vals_in ? p.vals_in[idx] : idx) : 0u;
+  }
   // where each digit starts in the whole output
   uint32_t unused;
   sm.global_base[threadIdx.x] = block_exclusive_scan(p.hist[threadIdx.x], sm.scan_tmp, unused);
 
-  // load (warp-striped) and rank within the warp; match.any groups equal digits and the lanes
-  // of a group are ranked in lane order, items in k order: a stable multi-split.
-  uint64_t key[kSortItems];
-  uint32_t val[kSortItems];
   uint32_t rank[kSortItems];
-  const uint32_t tile_base = tile * kSortTile + warp * (kSortItems * 32);
 #pragma unroll
   for (int k = 0; k < kSortItems; ++k) {
-    const uint32_t idx = tile_base + k * 32 + lane;
-    const bool valid = idx < R;
-    key[k] = valid ? p.keys_in[idx] : 0ull;
-    val[k] = valid ? p.vals_in[idx] : 0u;
-    const uint32_t digit = (uint32_t)(key[k] >> p.shift) & (kRadix - 1);
-    const unsigned peers = __match_any_sync(kFullMask, valid ? digit : (0x10000u + lane));
+    const bool valid = tile_base + k * 32 < n;
+    const uint32_t digit = (key[k] >> shift) & mask;
+    const unsigned peers = __match_any_sync(kFullMask, valid ? digit : (0x10000u | lane));
     const int leader = __ffs(peers) - 1;
     uint32_t old = 0;
     if (valid && lane == leader) {
@@ -212,16 +177,15 @@ __global__ void __launch_bounds__(kSortThreads) sort_pass_kernel(SortPassParams 
   sm.block_excl[d] = block_exclusive_scan(count, sm.scan_tmp, tile_items);
   __syncthreads();  // every digit's block-local start is read by other threads below
 
-  // decoupled look-back for this digit
+  // decoupled look-back for digit d (digits above the mask are empty everywhere)
   uint32_t* lb = p.lookback;
-  if (tile == 0) {
-    st_relaxed_u32(&lb[d], kLbPrefix | count);
+  if (tile == 0 || (uint32_t)d > mask) {
+    st_relaxed_u32(&lb[(size_t)tile * kRadix + d], kLbPrefix | count);
   } else {
     st_relaxed_u32(&lb[(size_t)tile * kRadix + d], kLbAggregate | count);
     uint32_t prev = 0;
     int64_t j = (int64_t)tile - 1;
-    bool gave_up = false;
-    bool found = false;
+    bool gave_up = false, found = false;
     while (!found) {
       uint32_t w[kLookbackBatch];
 #pragma unroll
@@ -229,9 +193,8 @@ __global__ void __launch_bounds__(kSortThreads) sort_pass_kernel(SortPassParams 
         w[b] = (j - b >= 0) ? ld_relaxed_u32(&lb[(size_t)(j - b) * kRadix + d]) : kLbPrefix;
 #pragma unroll
       for (int b = 0; b < kLookbackBatch; ++b) {
-        if (found) break;
         uint32_t x = w[b];
-        if ((x >> 30) == 0) {
+        if (!found && (x >> 30) == 0) {
           int spins = 0;
           do {
             if (++spins > kMaxSpins) {
@@ -243,8 +206,10 @@ __global__ void __launch_bounds__(kSortThreads) sort_pass_kernel(SortPassParams 
             x = ld_relaxed_u32(&lb[(size_t)(j - b) * kRadix + d]);
           } while ((x >> 30) == 0);
         }
-        prev += x & kLbValue;
-        if ((x >> 30) == 2) found = true;
+        if (!found) {
+          prev += x & kLbValue;
+          found = (x >> 30) == 2;
+        }
       }
       j -= kLookbackBatch;
     }
@@ -253,11 +218,11 @@ __global__ void __launch_bounds__(kSortThreads) sort_pass_kernel(SortPassParams 
     sm.global_base[d] += prev;
   }
 
-  // scatter into shared memory in digit order
+  // reorder the tile in shared memory by digit
 #pragma unroll
   for (int k = 0; k < kSortItems; ++k) {
     if (rank[k] != 0xffffffffu) {
-      const uint32_t digit = (uint32_t)(key[k] >> p.shift) & (kRadix - 1);
+      const uint32_t digit = (key[k] >> shift) & mask;
       const uint32_t pos = sm.block_excl[digit] + sm.warp_hist[warp][digit] + rank[k];
       if (pos < (uint32_t)kSortTile) {  // always true: ranks are consistent within the block
         sm.keys[pos] = key[k];
@@ -266,65 +231,197 @@ __global__ void __launch_bounds__(kSortThreads) sort_pass_kernel(SortPassParams 
     }
   }
   __syncthreads();
-  // write runs of equal digits to their global positions
   for (uint32_t i = threadIdx.x; i < tile_items; i += kSortThreads) {
-    const uint64_t k64 = sm.keys[i];
-    const uint32_t digit = (uint32_t)(k64 >> p.shift) & (kRadix - 1);
+    const uint32_t k32 = sm.keys[i];
+    const uint32_t digit = (k32 >> shift) & mask;
     const uint32_t out = sm.global_base[digit] + (i - sm.block_excl[digit]);
-    if (out < R) {  // always true unless a look-back gave up (then the status word says so)
-      p.keys_out[out] = k64;
+    if (out < n) {  // always true unless a look-back gave up (the status word then says so)
+      p.keys_out[out] = k32;
       p.vals_out[out] = sm.vals[i];
     }
   }
 }
 
-__global__ void ranges_kernel(RangesParams p) {
-  if (!capacity_ok(p.hdr, p.capacity)) return;
-  const uint32_t L = p.hdr->num_rendered;
-  const uint32_t idx = blockIdx.x * blockDim.x + threadIdx.x;
-  if (idx >= L) return;
-  const uint32_t cur = (uint32_t)(p.keys[idx] >> 32);
-  if (cur >= p.num_tiles) return;  // keys always hold valid tile ids; never index past the table
-  if (idx == 0)
-    p.ranges[cur].x = 0;
-  else {
-    const uint32_t prev = (uint32_t)(p.keys[idx - 1] >> 32);
-    if (cur != prev) {
-      if (prev < p.num_tiles) p.ranges[prev].y = idx;
-      p.ranges[cur].x = idx;
+// ---------------------------------------------------------------- duplicate -------------------
+// duplicateWithKeys over the depth-sorted Gaussians, fused with the scan of their tile counts.
+// Block b takes sorted positions [256 b, 256 b + 256); its output offset comes from a block scan
+// plus a decoupled look-back over the preceding blocks.  Each warp then writes the instances of
+// its 32 Gaussians (one contiguous span) 32 at a time: a 5-step shuffle search finds each
+// instance's Gaussian, so a splat covering hundreds of tiles does not serialise one thread.
+__global__ void __launch_bounds__(kScanBlock) duplicate_kernel(DuplicateParams p) {
+  __shared__ uint32_t s_tile;
+  __shared__ uint32_t s_warp[kScanBlock / 32];
+  __shared__ unsigned long long s_excl;
+  if (!instances_fit(p.hdr, p.capacity)) {
+    if (blockIdx.x == 0 && threadIdx.x == 0) atomicOr(&p.hdr->status, kStatusCapacity);
+    return;
+  }
+  if (threadIdx.x == 0) s_tile = atomicAdd(&p.hdr->dup_tile_counter, 1u);
+  __syncthreads();
+  const uint32_t tile = s_tile;
+  const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
+  const uint32_t i = tile * kScanBlock + threadIdx.x;
+  uint32_t count = 0, g = 0;
+  int rminx = 0, rminy = 0, width = 1;
+  if (i < (uint32_t)p.P) {
+    g = p.order[i];
+    const int radius = (g < (uint32_t)p.P) ? p.radii[g] : 0;
+    if (radius > 0) {
+      const float4 a = p.splat[2 * g];
+      int2 rmin, rmax;
+      tile_rect(make_float2(a.x, a.y), radius, p.gx, p.gy, rmin, rmax);
+      rminx = rmin.x;
+      rminy = rmin.y;
+      width = rmax.x - rmin.x;
+      count = (uint32_t)width * (uint32_t)(rmax.y - rmin.y);
+      if (count == 0) width = 1;
     }
   }
-  if (idx == L - 1) p.ranges[cur].y = L;
+  // block inclusive scan of the counts
+  uint32_t v = count;
+#pragma unroll
+  for (int o = 1; o < 32; o <<= 1) {
+    const uint32_t n = __shfl_up_sync(kFullMask, v, o);
+    if (lane >= o) v += n;
+  }
+  if (lane == 31) s_warp[warp] = v;
+  __syncthreads();
+  if (warp == 0) {
+    uint32_t w = (lane < kScanBlock / 32) ? s_warp[lane] : 0u;
+#pragma unroll
+    for (int o = 1; o < kScanBlock / 32; o <<= 1) {
+      const uint32_t n = __shfl_up_sync(kFullMask, w, o);
+      if (lane >= o) w += n;
+    }
+    if (lane < kScanBlock / 32) s_warp[lane] = w;
+  }
+  __syncthreads();
+  const uint32_t incl_local = v + (warp > 0 ? s_warp[warp - 1] : 0u);
+  const unsigned long long block_total = s_warp[kScanBlock / 32 - 1];
+  // decoupled look-back across blocks (warp 0)
+  if (warp == 0) {
+    if (tile == 0) {
+      if (lane == 0) {
+        st_relaxed_u64(&p.scan_state[0], kScanPrefix | block_total);
+        s_excl = 0;
+      }
+    } else {
+      if (lane == 0) st_relaxed_u64(&p.scan_state[tile], kScanAggregate | block_total);
+      unsigned long long excl = 0;
+      long long base = (long long)tile - 1;
+      bool gave_up = false;
+      for (;;) {
+        const long long j = base - lane;
+        unsigned long long w = kScanPrefix;  // virtual zero prefix before the first block
+        if (j >= 0) {
+          w = ld_relaxed_u64(&p.scan_state[j]);
+          int spins = 0;
+          while ((w >> 62) == 0) {
+            if (++spins > kMaxSpins) {
+              gave_up = true;
+              w = kScanPrefix;
+              break;
+            }
+            __nanosleep(64);
+            w = ld_relaxed_u64(&p.scan_state[j]);
+          }
+        }
+        const unsigned prefix_lanes = __ballot_sync(kFullMask, (w >> 62) == 2);
+        const int stop = prefix_lanes ? (__ffs(prefix_lanes) - 1) : 31;
+        unsigned long long c = (lane <= stop) ? (w & kScanValue) : 0ull;
+#pragma unroll
+        for (int o = 16; o > 0; o >>= 1) c += __shfl_xor_sync(kFullMask, c, o);
+        excl += c;
+        if (prefix_lanes) break;
+        base -= 32;
+      }
+      if (__any_sync(kFullMask, gave_up) && lane == 0) atomicOr(&p.hdr->status, kStatusLookback);
+      if (lane == 0) {
+        st_relaxed_u64(&p.scan_state[tile], kScanPrefix | ((excl + block_total) & kScanValue));
+        s_excl = excl;
+      }
+    }
+  }
+  __syncthreads();
+  const uint32_t start = (uint32_t)(s_excl + incl_local - count);
+  const uint32_t last_tile = (uint32_t)((p.P + kScanBlock - 1) / kScanBlock) - 1u;
+  if (tile == last_tile && threadIdx.x == kScanBlock - 1 && s_excl + block_total != p.hdr->num_rendered64)
+    atomicOr(&p.hdr->status, kStatusInconsistent);
+
+  // emit this warp's instances
+  const uint32_t w_begin = __shfl_sync(kFullMask, start, 0);
+  const uint32_t w_end = __shfl_sync(kFullMask, start + count, 31);
+  const uint32_t limit = (uint32_t)min((long long)p.capacity, 0xffffffffll);
+  for (uint32_t o0 = w_begin; o0 < w_end; o0 += 32) {
+    const uint32_t o = o0 + lane;
+    int pos = 0;
+#pragma unroll
+    for (int step = 16; step > 0; step >>= 1) {
+      const uint32_t s = __shfl_sync(kFullMask, start, pos + step);
+      if (s <= o) pos += step;
+    }
+    const uint32_t o_start = __shfl_sync(kFullMask, start, pos);
+    const int o_rminx = __shfl_sync(kFullMask, rminx, pos);
+    const int o_rminy = __shfl_sync(kFullMask, rminy, pos);
+    const int o_width = __shfl_sync(kFullMask, width, pos);
+    const uint32_t o_g = __shfl_sync(kFullMask, g, pos);
+    if (o < w_end && o < limit) {
+      const uint32_t local = o - o_start;
+      const uint32_t ty = (uint32_t)o_rminy + local / (uint32_t)o_width;
+      const uint32_t tx = (uint32_t)o_rminx + local % (uint32_t)o_width;
+      p.tkeys[o] = ty * (uint32_t)p.gx + tx;
+      p.tvals[o] = o_g;
+    }
+  }
+}
+
+// ---------------------------------------------------------------- tile ranges -----------------
+__global__ void ranges_kernel(RangesParams p) {
+  const uint32_t L = item_count(p.hdr, 0u, p.capacity);
+  for (uint32_t idx = blockIdx.x * blockDim.x + threadIdx.x; idx < L; idx += gridDim.x * blockDim.x) {
+    const uint32_t cur = p.keys[idx];
+    if (cur >= p.num_tiles) continue;  // keys always hold valid tile ids; never index past the table
+    if (idx == 0)
+      p.ranges[cur].x = 0;
+    else {
+      const uint32_t prev = p.keys[idx - 1];
+      if (cur != prev) {
+        if (prev < p.num_tiles) p.ranges[prev].y = idx;
+        p.ranges[cur].x = idx;
+      }
+    }
+    if (idx == L - 1) p.ranges[cur].y = L;
+  }
+}
+
+int sm_count() {
+  int dev = 0, sms = 148;
+  cudaGetDevice(&dev);
+  cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev);
+  return sms;
 }
 
 }  // namespace
 
-void launch_duplicate(const DuplicateParams& p, cudaStream_t s) {
-  if (p.P <= 0) return;
-  int dev = 0, sms = 148;
-  cudaGetDevice(&dev);
-  cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev);
-  const int warps_needed = (p.P + 31) / 32;
-  const int blocks = std::max(1, std::min((warps_needed + 7) / 8, sms * 8));
-  duplicate_kernel<<<blocks, kDupThreads, 0, s>>>(p);
+void launch_histogram(const HistParams& p, int64_t max_items, cudaStream_t s) {
+  const int64_t blocks = std::max<int64_t>(1, std::min<int64_t>((max_items + 255) / 256, sm_count() * 4));
+  histogram_kernel<<<(unsigned)blocks, 256, 0, s>>>(p);
 }
 
-void launch_sort_pass(const SortPassParams& p, cudaStream_t s) {
-  static bool configured[64] = {};
-  int dev = 0;
-  cudaGetDevice(&dev);
-  if (dev < 0 || dev >= 64 || !configured[dev]) {
-    cudaFuncSetAttribute(sort_pass_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)sizeof(SortSmem));
-    if (dev >= 0 && dev < 64) configured[dev] = true;
-  }
-  const int64_t blocks = BinningLayout::sort_tiles(p.capacity);
+void launch_onesweep(const OnesweepParams& p, int64_t max_items, cudaStream_t s) {
+  const int64_t blocks = sort_tiles(max_items);
   if (blocks <= 0) return;
-  sort_pass_kernel<<<(unsigned)blocks, kSortThreads, sizeof(SortSmem), s>>>(p);
+  onesweep_kernel<<<(unsigned)blocks, kSortThreads, 0, s>>>(p);
+}
+
+void launch_duplicate(const DuplicateParams& p, cudaStream_t s) {
+  if (p.P <= 0) return;
+  duplicate_kernel<<<(p.P + kScanBlock - 1) / kScanBlock, kScanBlock, 0, s>>>(p);
 }
 
 void launch_ranges(const RangesParams& p, cudaStream_t s) {
   if (p.capacity <= 0) return;
-  const int64_t blocks = (p.capacity + 255) / 256;
+  const int64_t blocks = std::max<int64_t>(1, std::min<int64_t>((p.capacity + 255) / 256, sm_count() * 8));
   ranges_kernel<<<(unsigned)blocks, 256, 0, s>>>(p);
 }
 

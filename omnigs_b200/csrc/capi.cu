@@ -78,11 +78,8 @@ void staged(int stage, int kernels, cudaStream_t s, F&& launch) {
   g_timed.push_back(t);
 }
 
-int sort_passes(int W, int H) {
-  const uint32_t tiles = (uint32_t)tiles_x(W) * (uint32_t)tiles_y(H);
-  const int bits = 32 + (int)higher_msb(tiles);
-  return (bits + kRadixBits - 1) / kRadixBits;
-}
+// Buffer (0 or 1) that holds the sorted tile ids / point list after the tile passes.
+int tile_final(int W, int H) { return TileDigits::make(W, H).passes & 1; }
 
 int validate_common(int P, int D, int M, int W, int H, const float* shs, const float* colors,
                     const float* scales, const float* rotations, const float* cov3D,
@@ -119,7 +116,11 @@ int validate_forward(const OmnigsLonlatForwardArgs* a) {
 }
 
 __global__ void begin_render_kernel(GeomHeader* hdr) {
-  atomicAnd(&hdr->status, ~kStatusCapacity);
+  atomicAnd(&hdr->status, ~(kStatusCapacity | kStatusInconsistent));
+  const unsigned long long total = hdr->num_rendered64;
+  if (total > (unsigned long long)kMaxInstances) atomicOr(&hdr->status, kStatusOverflow);
+  hdr->num_rendered = (uint32_t)(total > 0xffffffffull ? 0xffffffffull : total);
+  hdr->dup_tile_counter = 0;
   for (int i = 0; i < kMaxSortPasses; ++i) hdr->sort_tile_counter[i] = 0;
 }
 
@@ -180,7 +181,7 @@ int omnigs_lonlat_preprocess(const OmnigsLonlatForwardArgs* a, void* geom, size_
   const GeomLayout L = GeomLayout::make(a->P);
   if (geom == nullptr || geom_bytes < L.total)
     return fail(OMNIGS_ERR_BUFFER_TOO_SMALL, "geometry buffer smaller than omnigs_lonlat_geom_bytes(P)");
-  if (cudaMemsetAsync(geom, 0, L.zero_end, s) != cudaSuccess) return check_launch("memset geometry header");
+  if (cudaMemsetAsync(geom, 0, sizeof(GeomHeader), s) != cudaSuccess) return check_launch("memset geometry header");
   if (a->P == 0) return OMNIGS_OK;
   PreprocessParams p{};
   p.P = a->P;
@@ -204,9 +205,8 @@ int omnigs_lonlat_preprocess(const OmnigsLonlatForwardArgs* a, void* geom, size_
   p.splat = at<float4>(geom, L.splat);
   p.color = at<float4>(geom, L.color);
   p.depth = at<float>(geom, L.depth);
-  p.offsets = at<uint32_t>(geom, L.offsets);
+  p.tiles_touched = at<uint32_t>(geom, L.tiles_touched);
   p.grad_acc = at<float4>(geom, L.grad_acc);
-  p.scan_state = at<unsigned long long>(geom, L.scan_state);
   p.hdr = at<GeomHeader>(geom, L.header);
   staged(OMNIGS_STAGE_PREPROCESS, 1, s, [&] { launch_preprocess(p, s); });
   return check_launch("preprocess");
@@ -232,62 +232,109 @@ int omnigs_lonlat_render(const OmnigsLonlatForwardArgs* a, void* geom, size_t ge
     return fail(OMNIGS_ERR_BUFFER_TOO_SMALL, "geometry buffer smaller than omnigs_lonlat_geom_bytes(P)");
   if (image == nullptr || image_bytes < IL.total)
     return fail(OMNIGS_ERR_BUFFER_TOO_SMALL, "image buffer smaller than omnigs_lonlat_image_bytes(W, H)");
-  const int64_t capacity = BinningLayout::capacity_for(binning_bytes);
+  int64_t capacity = BinningLayout::capacity_for(binning_bytes);
   if (binning == nullptr || capacity < 0)
     return fail(OMNIGS_ERR_BUFFER_TOO_SMALL, "binning buffer smaller than omnigs_lonlat_binning_bytes(0)");
   const BinningLayout BL = BinningLayout::make(capacity);
+  if (capacity > kMaxInstances) capacity = kMaxInstances;
   const int gx = tiles_x(a->W), gy = tiles_y(a->H);
-  const int passes = sort_passes(a->W, a->H);
+  const TileDigits td = TileDigits::make(a->W, a->H);
   GeomHeader* hdr = at<GeomHeader>(geom, GL.header);
   uint32_t* hist = at<uint32_t>(binning, BL.hist);
-  uint32_t* lookback = at<uint32_t>(binning, BL.lookback);
   uint2* ranges = at<uint2>(image, IL.ranges);
+  const int64_t depth_tiles = sort_tiles(a->P);
+  const int64_t inst_tiles = sort_tiles(BL.capacity);
 
   staged(OMNIGS_STAGE_OTHER, 1, s, [&] { begin_render_kernel<<<1, 1, 0, s>>>(hdr); });
-  if (cudaMemsetAsync(hist, 0, sizeof(uint32_t) * kMaxSortPasses * kRadix, s) != cudaSuccess ||
+  if (cudaMemsetAsync(at<unsigned char>(geom, GL.dup_scan), 0, GL.zero_end - GL.dup_scan, s) != cudaSuccess ||
+      cudaMemsetAsync(hist, 0, sizeof(uint32_t) * kMaxSortPasses * kRadix, s) != cudaSuccess ||
+      cudaMemsetAsync(at<uint32_t>(binning, BL.tile_lookback), 0,
+                      sizeof(uint32_t) * td.passes * inst_tiles * kRadix, s) != cudaSuccess ||
       cudaMemsetAsync(ranges, 0, sizeof(uint2) * (size_t)gx * gy, s) != cudaSuccess)
     return check_launch("memset binning state");
 
+  // 1. depth sort of the Gaussians: (depth bits, index) order
+  const uint32_t* depth_keys = at<uint32_t>(geom, GL.depth);
+  uint32_t* dkeys[2] = {at<uint32_t>(geom, GL.dkeys0), at<uint32_t>(geom, GL.dkeys1)};
+  uint32_t* dvals[2] = {at<uint32_t>(geom, GL.dvals0), at<uint32_t>(geom, GL.dvals1)};
+  HistParams hd{};
+  hd.keys = depth_keys;
+  hd.n_host = (uint32_t)a->P;
+  hd.passes = kDepthPasses;
+  for (int q = 0; q < kDepthPasses; ++q) {
+    hd.shift[q] = kRadixBits * q;
+    hd.mask[q] = kRadix - 1;
+  }
+  hd.hist = hist;
+  staged(OMNIGS_STAGE_SORT, 1, s, [&] { launch_histogram(hd, a->P, s); });
+  for (int q = 0; q < kDepthPasses; ++q) {
+    OnesweepParams op{};
+    op.keys_in = q == 0 ? depth_keys : dkeys[(q + 1) & 1];
+    op.vals_in = q == 0 ? nullptr : dvals[(q + 1) & 1];
+    op.keys_out = dkeys[q & 1];
+    op.vals_out = dvals[q & 1];
+    op.shift = kRadixBits * q;
+    op.mask = kRadix - 1;
+    op.n_host = (uint32_t)a->P;
+    op.hist = hist + q * kRadix;
+    op.lookback = at<uint32_t>(geom, GL.depth_lookback) + (size_t)q * depth_tiles * kRadix;
+    op.tile_counter = &hdr->sort_tile_counter[q];
+    op.hdr = hdr;
+    staged(OMNIGS_STAGE_SORT, 1, s, [&] { launch_onesweep(op, a->P, s); });
+  }
+  const uint32_t* order = dvals[(kDepthPasses - 1) & 1];
+
+  // 2. duplicate in that order (fused scan of the tile counts)
+  uint32_t* tkeys[2] = {at<uint32_t>(binning, BL.tkeys0), at<uint32_t>(binning, BL.tkeys1)};
+  uint32_t* tvals[2] = {at<uint32_t>(binning, BL.tvals0), at<uint32_t>(binning, BL.tvals1)};
   DuplicateParams d{};
   d.P = a->P;
   d.gx = gx;
   d.gy = gy;
-  d.passes = passes;
   d.radii = a->radii;
   d.splat = at<float4>(geom, GL.splat);
-  d.depth = at<float>(geom, GL.depth);
-  d.offsets = at<uint32_t>(geom, GL.offsets);
-  d.keys = at<uint64_t>(binning, BL.keys0);
-  d.vals = at<uint32_t>(binning, BL.vals0);
-  d.hist = hist;
-  d.lookback = lookback;
-  d.lookback_pass_stride = BinningLayout::sort_tiles(capacity) * kRadix;
+  d.order = order;
+  d.tkeys = tkeys[0];
+  d.tvals = tvals[0];
+  d.scan_state = at<unsigned long long>(geom, GL.dup_scan);
   d.capacity = capacity;
   d.hdr = hdr;
   staged(OMNIGS_STAGE_DUPLICATE, 1, s, [&] { launch_duplicate(d, s); });
-  if (int rc = check_launch("duplicate")) return rc;
 
-  uint64_t* keys[2] = {at<uint64_t>(binning, BL.keys0), at<uint64_t>(binning, BL.keys1)};
-  uint32_t* vals[2] = {at<uint32_t>(binning, BL.vals0), at<uint32_t>(binning, BL.vals1)};
-  for (int pass = 0; pass < passes; ++pass) {
-    SortPassParams sp{};
-    sp.keys_in = keys[pass & 1];
-    sp.vals_in = vals[pass & 1];
-    sp.keys_out = keys[(pass + 1) & 1];
-    sp.vals_out = vals[(pass + 1) & 1];
-    sp.hist = hist + pass * kRadix;
-    sp.lookback = lookback + pass * d.lookback_pass_stride;
-    sp.tile_counter = &hdr->sort_tile_counter[pass];
-    sp.shift = kRadixBits * pass;
-    sp.capacity = capacity;
-    sp.hdr = hdr;
-    staged(OMNIGS_STAGE_SORT, 1, s, [&] { launch_sort_pass(sp, s); });
-    if (int rc = check_launch("sort pass")) return rc;
+  // 3. stable tile sort of the instances
+  HistParams ht{};
+  ht.keys = tkeys[0];
+  ht.count_hdr = hdr;
+  ht.capacity = capacity;
+  ht.passes = td.passes;
+  for (int q = 0; q < td.passes; ++q) {
+    ht.shift[q] = td.shift[q];
+    ht.mask[q] = td.mask[q];
   }
-  const int fin = passes & 1;
+  ht.hist = hist + kDepthPasses * kRadix;
+  staged(OMNIGS_STAGE_SORT, 1, s, [&] { launch_histogram(ht, capacity, s); });
+  for (int q = 0; q < td.passes; ++q) {
+    OnesweepParams op{};
+    op.keys_in = tkeys[q & 1];
+    op.vals_in = tvals[q & 1];
+    op.keys_out = tkeys[(q + 1) & 1];
+    op.vals_out = tvals[(q + 1) & 1];
+    op.shift = td.shift[q];
+    op.mask = td.mask[q];
+    op.count_hdr = hdr;
+    op.capacity = capacity;
+    op.hist = hist + (kDepthPasses + q) * kRadix;
+    op.lookback = at<uint32_t>(binning, BL.tile_lookback) + (size_t)q * inst_tiles * kRadix;
+    op.tile_counter = &hdr->sort_tile_counter[kDepthPasses + q];
+    op.hdr = hdr;
+    staged(OMNIGS_STAGE_SORT, 1, s, [&] { launch_onesweep(op, capacity, s); });
+  }
+  const int fin = td.passes & 1;
+  if (int rc = check_launch("binning")) return rc;
 
+  // 4. tile ranges
   RangesParams rp{};
-  rp.keys = keys[fin];
+  rp.keys = tkeys[fin];
   rp.ranges = ranges;
   rp.num_tiles = (uint32_t)gx * (uint32_t)gy;
   rp.capacity = capacity;
@@ -302,7 +349,7 @@ int omnigs_lonlat_render(const OmnigsLonlatForwardArgs* a, void* geom, size_t ge
   r.gx = gx;
   r.gy = gy;
   r.ranges = ranges;
-  r.point_list = vals[fin];
+  r.point_list = tvals[fin];
   r.capacity = capacity;
   r.splat = at<float4>(geom, GL.splat);
   r.color = at<float4>(geom, GL.color);
@@ -362,7 +409,7 @@ int omnigs_lonlat_backward(const OmnigsLonlatBackwardArgs* a, void* geom, size_t
   if (a->R > capacity) return fail(OMNIGS_ERR_CAPACITY, "R exceeds the binning buffer's capacity");
   const BinningLayout BL = BinningLayout::make(capacity);
   const int gx = tiles_x(a->W), gy = tiles_y(a->H);
-  const int fin = sort_passes(a->W, a->H) & 1;
+  const int fin = tile_final(a->W, a->H);
 
   RenderParams r{};
   r.P = a->P;
@@ -371,7 +418,7 @@ int omnigs_lonlat_backward(const OmnigsLonlatBackwardArgs* a, void* geom, size_t
   r.gx = gx;
   r.gy = gy;
   r.ranges = at<uint2>(image, IL.ranges);
-  r.point_list = at<uint32_t>(binning, fin ? BL.vals1 : BL.vals0);
+  r.point_list = at<uint32_t>(binning, fin ? BL.tvals1 : BL.tvals0);
   r.capacity = capacity;
   r.splat = at<float4>(geom, GL.splat);
   r.color = at<float4>(geom, GL.color);
@@ -462,7 +509,8 @@ int omnigs_lonlat_geom_view(const void* geom, int P, OmnigsLonlatGeomView* out) 
   out->splat = at<float>(geom, L.splat);
   out->color = at<float>(geom, L.color);
   out->depth = at<float>(geom, L.depth);
-  out->offsets = at<uint32_t>(geom, L.offsets);
+  out->tiles_touched = at<uint32_t>(geom, L.tiles_touched);
+  out->depth_order = at<uint32_t>(geom, (kDepthPasses - 1) & 1 ? L.dvals1 : L.dvals0);
   return OMNIGS_OK;
 }
 
@@ -473,9 +521,9 @@ int omnigs_lonlat_binning_view(const void* binning, size_t binning_bytes, int W,
   const int64_t capacity = BinningLayout::capacity_for(binning_bytes);
   if (capacity < 0) return fail(OMNIGS_ERR_BUFFER_TOO_SMALL, "binning buffer too small");
   const BinningLayout L = BinningLayout::make(capacity);
-  const int fin = sort_passes(W, H) & 1;
-  out->keys = at<uint64_t>(binning, fin ? L.keys1 : L.keys0);
-  out->point_list = at<uint32_t>(binning, fin ? L.vals1 : L.vals0);
+  const int fin = tile_final(W, H);
+  out->tile_ids = at<uint32_t>(binning, fin ? L.tkeys1 : L.tkeys0);
+  out->point_list = at<uint32_t>(binning, fin ? L.tvals1 : L.tvals0);
   return OMNIGS_OK;
 }
 

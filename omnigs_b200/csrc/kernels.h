@@ -23,47 +23,59 @@ struct PreprocessParams {
   int* radii;
   float4* splat;
   float4* color;
-  float* depth;
-  uint32_t* offsets;
+  float* depth;              // [P] radial depth; +inf for culled Gaussians (depth-sort key)
+  uint32_t* tiles_touched;   // [P]
   float4* grad_acc;
-  unsigned long long* scan_state;
-  GeomHeader* hdr;
+  GeomHeader* hdr;           // num_rendered64 is accumulated here
+};
+
+// Digit histograms of up to kDepthPasses digits of u32 keys.
+struct HistParams {
+  const uint32_t* keys;
+  uint32_t n_host;             // item count when count_hdr is null
+  const GeomHeader* count_hdr; // else the device num_rendered (0 if over capacity)
+  int64_t capacity;
+  int passes;
+  int shift[kDepthPasses];
+  uint32_t mask[kDepthPasses];
+  uint32_t* hist;              // [passes][kRadix], zeroed by the caller
+};
+
+// One stable LSD radix pass over (u32 key, u32 value) pairs.
+struct OnesweepParams {
+  const uint32_t* keys_in;
+  const uint32_t* vals_in;     // null: the value is the item index
+  uint32_t* keys_out;
+  uint32_t* vals_out;
+  int shift;
+  uint32_t mask;
+  uint32_t n_host;
+  const GeomHeader* count_hdr;
+  int64_t capacity;
+  const uint32_t* hist;        // this pass's [kRadix] histogram
+  uint32_t* lookback;          // [sort tiles][kRadix], zeroed by the caller
+  uint32_t* tile_counter;      // zeroed by the caller
+  GeomHeader* hdr;             // status bits
 };
 
 struct DuplicateParams {
-  int P, gx, gy, passes, last_pass_bits;
+  int P, gx, gy;
   const int* radii;
   const float4* splat;
-  const float* depth;
-  const uint32_t* offsets;
-  uint64_t* keys;
-  uint32_t* vals;
-  uint32_t* hist;      // [kMaxSortPasses][kRadix], zeroed by the caller
-  uint32_t* lookback;  // [kMaxSortPasses][sort tiles][kRadix], cleared here for the tiles in use
-  int64_t lookback_pass_stride;
+  const uint32_t* order;       // [P] Gaussian indices sorted by (depth bits, index)
+  uint32_t* tkeys;             // [capacity] tile ids
+  uint32_t* tvals;             // [capacity] Gaussian indices
+  unsigned long long* scan_state;
   int64_t capacity;
   GeomHeader* hdr;
-};
-
-struct SortPassParams {
-  const uint64_t* keys_in;
-  const uint32_t* vals_in;
-  uint64_t* keys_out;
-  uint32_t* vals_out;
-  const uint32_t* hist;   // this pass's [kRadix] digit histogram
-  uint32_t* lookback;     // this pass's [sort tiles][kRadix] look-back words
-  uint32_t* tile_counter;
-  int shift;
-  int64_t capacity;
-  GeomHeader* hdr;        // reads num_rendered / status, sets status bits
 };
 
 struct RangesParams {
-  const uint64_t* keys;
+  const uint32_t* keys;        // sorted tile ids
   uint2* ranges;
   uint32_t num_tiles;
   int64_t capacity;
-  GeomHeader* hdr;
+  const GeomHeader* hdr;
 };
 
 struct RenderParams {
@@ -107,12 +119,14 @@ struct PreprocessBackwardParams {
 };
 
 void launch_preprocess(const PreprocessParams& p, cudaStream_t s);
+void launch_histogram(const HistParams& p, int64_t max_items, cudaStream_t s);
+void launch_onesweep(const OnesweepParams& p, int64_t max_items, cudaStream_t s);
 void launch_duplicate(const DuplicateParams& p, cudaStream_t s);
-void launch_sort_pass(const SortPassParams& p, cudaStream_t s);
 void launch_ranges(const RangesParams& p, cudaStream_t s);
 void launch_render_forward(const RenderParams& p, cudaStream_t s);
 void launch_render_backward(const RenderParams& p, cudaStream_t s);
 void launch_preprocess_backward(const PreprocessBackwardParams& p, cudaStream_t s);
+
 // Sets the message returned by omnigs_last_error() on this host thread.
 void set_last_error(const char* msg);
 

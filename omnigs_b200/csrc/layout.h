@@ -4,15 +4,17 @@
 // (cuda_rasterizer/rasterizer_impl.h:37-102).  The buffers stay opaque at the API, so this
 // library lays them out for its own kernels:
 //
-//   geometry (per Gaussian, P):  header | scan look-back u64[scan tiles] |
+//   geometry (per Gaussian, P):  header | duplicate-scan look-back u64[P/256] |
+//                                depth-sort look-back u32[4][sort tiles][256] |
 //                                splat records float4[2P] {x, y, conic a, b}
 //                                {conic c, opacity, cull half-width, cull half-height} |
 //                                colour float4[P] {r, g, b, clamp bits} | depth f32[P] |
-//                                inclusive tile offsets u32[P] | gradient accumulators float4[3P]
+//                                tiles_touched u32[P] | depth-sort keys/values u32[4][P] |
+//                                gradient accumulators float4[3P]
 //   image (per pixel, N = W*H):  final transmittance f32[N] | last contributor u32[N] |
 //                                tile ranges uint2[tiles]
-//   binning (per instance, capacity C): keys u64[2][C] | values u32[2][C] |
-//                                digit histograms u32[8][256] | sort look-back u32[8][sort tiles][256]
+//   binning (per instance, capacity C): tile keys u32[2][C] | Gaussian indices u32[2][C] |
+//                                digit histograms u32[7][256] | tile-sort look-back u32[3][tiles][256]
 //
 // Every array starts on a 256-byte boundary.
 #pragma once
@@ -20,52 +22,67 @@
 #include <cstddef>
 #include <cstdint>
 
+#if defined(__CUDACC__)
+#define OMNIGS_HD __host__ __device__
+#else
+#define OMNIGS_HD
+#endif
+
 namespace omnigs {
 
 constexpr size_t kAlign = 256;
-constexpr int kScanBlock = 256;          // Gaussians per preprocess block (one scan tile)
+constexpr int kScanBlock = 256;          // Gaussians per preprocess / duplicate block
 constexpr int kSortThreads = 256;
 constexpr int kSortItems = 16;           // keys per thread per sort tile
 constexpr int kSortTile = kSortThreads * kSortItems;
 constexpr int kRadixBits = 8;
 constexpr int kRadix = 1 << kRadixBits;
-constexpr int kMaxSortPasses = 8;        // 64-bit keys
+constexpr int kDepthPasses = 4;          // 32-bit depth keys, 8-bit digits
+constexpr int kTilePasses = 3;           // tile ids (<= 21 bits): up to three digits of <= 8 bits
+constexpr int kMaxSortPasses = kDepthPasses + kTilePasses;
 constexpr int64_t kMaxInstances = (int64_t(1) << 30) - 1;  // look-back words hold 30-bit counts
 
 // Device status bits, in GeomHeader::status.
 constexpr uint32_t kStatusCapacity = 1u;      // num_rendered exceeded the binning capacity
 constexpr uint32_t kStatusLookback = 2u;      // a bounded look-back wait gave up
 constexpr uint32_t kStatusOverflow = 4u;      // instance count does not fit the 30-bit counters
+constexpr uint32_t kStatusInconsistent = 8u;  // the duplicate pass counted a different total
 
 struct GeomHeader {
   uint32_t status;
   uint32_t num_rendered;
-  uint32_t scan_tile_counter;
+  uint32_t dup_tile_counter;
   uint32_t pad0;
-  uint64_t num_rendered64;
+  unsigned long long num_rendered64;
   uint32_t sort_tile_counter[kMaxSortPasses];
   uint32_t reserved[64 - 6 - kMaxSortPasses];
 };
 static_assert(sizeof(GeomHeader) == 256, "header must be 256 bytes");
 
-__host__ __device__ inline size_t align_up(size_t v) { return (v + kAlign - 1) / kAlign * kAlign; }
+OMNIGS_HD inline size_t align_up(size_t v) { return (v + kAlign - 1) / kAlign * kAlign; }
 
 inline int tiles_x(int W) { return (W + 15) / 16; }
 inline int tiles_y(int H) { return (H + 15) / 16; }
+inline int64_t sort_tiles(int64_t n) { return (n + kSortTile - 1) / kSortTile; }
 
 struct GeomLayout {
-  size_t header, scan_state, zero_end, splat, color, depth, offsets, grad_acc, total;
+  size_t header, dup_scan, depth_lookback, zero_end, splat, color, depth, tiles_touched, dkeys0,
+      dkeys1, dvals0, dvals1, grad_acc, total;
   static GeomLayout make(int64_t P) {
     GeomLayout L;
     size_t o = 0;
     L.header = o; o = align_up(o + sizeof(GeomHeader));
-    const int64_t scan_tiles = (P + kScanBlock - 1) / kScanBlock;
-    L.scan_state = o; o = align_up(o + sizeof(uint64_t) * scan_tiles);
-    L.zero_end = o;  // header and scan state are cleared together before each preprocess
+    L.dup_scan = o; o = align_up(o + sizeof(uint64_t) * ((P + kScanBlock - 1) / kScanBlock));
+    L.depth_lookback = o; o = align_up(o + sizeof(uint32_t) * kDepthPasses * sort_tiles(P) * kRadix);
+    L.zero_end = o;  // everything above is cleared before each preprocess
     L.splat = o; o = align_up(o + sizeof(float) * 8 * P);
     L.color = o; o = align_up(o + sizeof(float) * 4 * P);
     L.depth = o; o = align_up(o + sizeof(float) * P);
-    L.offsets = o; o = align_up(o + sizeof(uint32_t) * P);
+    L.tiles_touched = o; o = align_up(o + sizeof(uint32_t) * P);
+    L.dkeys0 = o; o = align_up(o + sizeof(uint32_t) * P);
+    L.dkeys1 = o; o = align_up(o + sizeof(uint32_t) * P);
+    L.dvals0 = o; o = align_up(o + sizeof(uint32_t) * P);
+    L.dvals1 = o; o = align_up(o + sizeof(uint32_t) * P);
     L.grad_acc = o; o = align_up(o + sizeof(float) * 12 * P);
     L.total = o;
     return L;
@@ -88,19 +105,18 @@ struct ImageLayout {
 };
 
 struct BinningLayout {
-  size_t keys0, keys1, vals0, vals1, hist, lookback, total;
+  size_t tkeys0, tkeys1, tvals0, tvals1, hist, tile_lookback, total;
   int64_t capacity;
-  static int64_t sort_tiles(int64_t capacity) { return (capacity + kSortTile - 1) / kSortTile; }
   static BinningLayout make(int64_t C) {
     BinningLayout L;
     L.capacity = C;
     size_t o = 0;
-    L.keys0 = o; o = align_up(o + sizeof(uint64_t) * C);
-    L.keys1 = o; o = align_up(o + sizeof(uint64_t) * C);
-    L.vals0 = o; o = align_up(o + sizeof(uint32_t) * C);
-    L.vals1 = o; o = align_up(o + sizeof(uint32_t) * C);
+    L.tkeys0 = o; o = align_up(o + sizeof(uint32_t) * C);
+    L.tkeys1 = o; o = align_up(o + sizeof(uint32_t) * C);
+    L.tvals0 = o; o = align_up(o + sizeof(uint32_t) * C);
+    L.tvals1 = o; o = align_up(o + sizeof(uint32_t) * C);
     L.hist = o; o = align_up(o + sizeof(uint32_t) * kMaxSortPasses * kRadix);
-    L.lookback = o; o = align_up(o + sizeof(uint32_t) * kMaxSortPasses * sort_tiles(C) * kRadix);
+    L.tile_lookback = o; o = align_up(o + sizeof(uint32_t) * kTilePasses * sort_tiles(C) * kRadix);
     L.total = o;
     return L;
   }
@@ -119,8 +135,18 @@ struct BinningLayout {
   }
 };
 
-// Number of 8-bit LSD passes that cover key bits [0, 32 + bit), bit = getHigherMsb(tiles)
-// (rasterizer_impl.cu:47-62, 651-661).
+// getHigherMsb (rasterizer_impl.cu:47-62): the reference sorts key bits [0, 32 + bit), i.e. all
+// tile-id bits; the tile passes here cover the same `bit` bits (rasterizer_impl.cu:651-661).
+inline uint32_t higher_msb(uint32_t n);
+
+// Digits of the tile sort: `bit` tile-id bits split into passes of at most 8 bits.
+struct TileDigits {
+  int passes;
+  int shift[kTilePasses];
+  uint32_t mask[kTilePasses];
+  static TileDigits make(int W, int H);
+};
+
 inline uint32_t higher_msb(uint32_t n) {
   uint32_t msb = sizeof(n) * 4;
   uint32_t step = msb;
@@ -133,6 +159,22 @@ inline uint32_t higher_msb(uint32_t n) {
   }
   if (n >> msb) msb++;
   return msb;
+}
+
+inline TileDigits TileDigits::make(int W, int H) {
+  const uint32_t tiles = (uint32_t)tiles_x(W) * (uint32_t)tiles_y(H);
+  const int bit = (int)higher_msb(tiles);
+  TileDigits t{};
+  t.passes = (bit + kRadixBits - 1) / kRadixBits;
+  if (t.passes < 1) t.passes = 1;
+  int shift = 0;
+  for (int i = 0; i < t.passes; ++i) {
+    const int width = (bit - shift + (t.passes - i) - 1) / (t.passes - i);  // spread evenly
+    t.shift[i] = shift;
+    t.mask[i] = width >= 32 ? 0xffffffffu : ((1u << width) - 1u);
+    shift += width;
+  }
+  return t;
 }
 
 }  // namespace omnigs

@@ -1,12 +1,12 @@
-// Forward preprocess of lonlat splats fused with the inclusive scan of tiles_touched.
+// Forward preprocess of lonlat splats, one thread per Gaussian.
 //
-// One thread per Gaussian evaluates the reference's FP32 sequence (forward.cu:592-703): near cull
-// at r^2 <= 0.04, equirect projection, 3D and 2D covariance, conic, radius, clamped tile rect and
-// SH colour.  The block then scans its 256 tile counts and joins a single-pass decoupled look-back
-// across blocks (blocks take scan tiles in launch order from an atomic counter, so each block only
-// waits on blocks that are already running), writing the inclusive offsets that the reference
-// computes with a separate cub::DeviceScan::InclusiveSum (rasterizer_impl.cu:622-623).  The
-// instance total stays on the device: nothing is copied to the host here.
+// Evaluates the reference's FP32 sequence (forward.cu:592-703): near cull at r^2 <= 0.04,
+// equirect projection, 3D and 2D covariance, conic, radius, clamped tile rect and SH colour.
+// Outputs per Gaussian: radius, the 32-byte splat record and colour record read by the blend
+// kernels, the radial depth (+inf for culled Gaussians: it is the depth-sort key of the binning)
+// and tiles_touched; the instance total is summed on the device (block reduction + one atomic
+// per block), so nothing is copied to the host (the reference copies num_rendered back between
+// its scan and its duplication, rasterizer_impl.cu:622-628).
 //
 // Besides the reference's outputs, each visible splat gets the half-extents of the axis-aligned
 // box outside which its alpha is provably below 1/255; the blend kernels use them to skip a splat
@@ -17,10 +17,6 @@
 
 namespace omnigs {
 namespace {
-
-constexpr unsigned long long kFlagAggregate = 1ull << 62;
-constexpr unsigned long long kFlagPrefix = 2ull << 62;
-constexpr unsigned long long kValueMask = (1ull << 62) - 1;
 
 // Half-extents (pixels) of the box that contains every pixel where o * exp(power) can reach the
 // reference's 1/255 skip threshold (forward.cu:436-438).  power = -d^T Q d / 2 with Q the conic,
@@ -42,19 +38,15 @@ __device__ __forceinline__ float2 cull_half_extent(float a, float b, float c, fl
   return make_float2(__double2float_ru(hx), __double2float_ru(hy));
 }
 
-__global__ void __launch_bounds__(kScanBlock) preprocess_scan_kernel(PreprocessParams p) {
-  __shared__ uint32_t s_tile;
+__global__ void __launch_bounds__(kScanBlock) preprocess_kernel(PreprocessParams p) {
   __shared__ uint32_t s_warp[kScanBlock / 32];
-  __shared__ unsigned long long s_excl;
-  if (threadIdx.x == 0) s_tile = atomicAdd(&p.hdr->scan_tile_counter, 1u);
-  __syncthreads();
-  const uint32_t tile = s_tile;
-  const int idx = (int)(tile * kScanBlock + threadIdx.x);
+  const int idx = blockIdx.x * kScanBlock + threadIdx.x;
   const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
 
   uint32_t touched = 0;
   if (idx < p.P) {
     p.radii[idx] = 0;
+    float depth_key = __int_as_float(0x7f800000);  // culled Gaussians sort last
     const float* vm = p.viewmatrix;
     const float3 p_orig = {p.means3D[3 * idx], p.means3D[3 * idx + 1], p.means3D[3 * idx + 2]};
     // near cull, auxiliary.h:198-220 (no frustum test for lonlat)
@@ -117,7 +109,7 @@ __global__ void __launch_bounds__(kScanBlock) preprocess_scan_kernel(PreprocessP
           p.splat[2 * idx] = make_float4(point_image.x, point_image.y, conic.x, conic.y);
           p.splat[2 * idx + 1] = make_float4(conic.z, opacity, ext.x, ext.y);
           p.color[idx] = col;
-          p.depth[idx] = r;
+          depth_key = r;
           p.radii[idx] = radius;
           const float4 z4 = make_float4(0.f, 0.f, 0.f, 0.f);
           p.grad_acc[3 * idx] = z4;
@@ -127,83 +119,21 @@ __global__ void __launch_bounds__(kScanBlock) preprocess_scan_kernel(PreprocessP
         }
       }
     }
+    p.depth[idx] = depth_key;
+    p.tiles_touched[idx] = touched;
   }
 
-  // ---- block-level inclusive scan of tiles_touched ----
+  // ---- instance total: block reduction, one atomic per block ----
   uint32_t v = touched;
 #pragma unroll
-  for (int o = 1; o < 32; o <<= 1) {
-    const uint32_t n = __shfl_up_sync(kFullMask, v, o);
-    if (lane >= o) v += n;
-  }
-  if (lane == 31) s_warp[warp] = v;
+  for (int o = 16; o > 0; o >>= 1) v += __shfl_xor_sync(kFullMask, v, o);
+  if (lane == 0) s_warp[warp] = v;
   __syncthreads();
-  if (warp == 0) {
-    uint32_t w = (lane < kScanBlock / 32) ? s_warp[lane] : 0u;
+  if (threadIdx.x == 0) {
+    unsigned long long total = 0;
 #pragma unroll
-    for (int o = 1; o < kScanBlock / 32; o <<= 1) {
-      const uint32_t n = __shfl_up_sync(kFullMask, w, o);
-      if (lane >= o) w += n;
-    }
-    if (lane < kScanBlock / 32) s_warp[lane] = w;
-  }
-  __syncthreads();
-  const uint32_t incl_local = v + (warp > 0 ? s_warp[warp - 1] : 0u);
-  const unsigned long long block_total = s_warp[kScanBlock / 32 - 1];
-
-  // ---- decoupled look-back across scan tiles (warp 0) ----
-  if (warp == 0) {
-    if (tile == 0) {
-      if (lane == 0) {
-        st_relaxed_u64(&p.scan_state[0], kFlagPrefix | block_total);
-        s_excl = 0;
-      }
-    } else {
-      if (lane == 0) st_relaxed_u64(&p.scan_state[tile], kFlagAggregate | block_total);
-      unsigned long long excl = 0;
-      long long base = (long long)tile - 1;
-      bool gave_up = false;
-      for (;;) {
-        const long long j = base - lane;
-        unsigned long long w = kFlagPrefix;  // virtual zero prefix before the first tile
-        if (j >= 0) {
-          w = ld_relaxed_u64(&p.scan_state[j]);
-          int spins = 0;
-          while ((w >> 62) == 0) {
-            if (++spins > kMaxSpins) {
-              gave_up = true;
-              w = kFlagPrefix;
-              break;
-            }
-            __nanosleep(64);
-            w = ld_relaxed_u64(&p.scan_state[j]);
-          }
-        }
-        const unsigned prefix_lanes = __ballot_sync(kFullMask, (w >> 62) == 2);
-        const int stop = prefix_lanes ? (__ffs(prefix_lanes) - 1) : 31;
-        unsigned long long c = (lane <= stop) ? (w & kValueMask) : 0ull;
-#pragma unroll
-        for (int o = 16; o > 0; o >>= 1) c += __shfl_xor_sync(kFullMask, c, o);
-        excl += c;
-        if (prefix_lanes) break;
-        base -= 32;
-      }
-      if (__any_sync(kFullMask, gave_up) && lane == 0) atomicOr(&p.hdr->status, kStatusLookback);
-      if (lane == 0) {
-        st_relaxed_u64(&p.scan_state[tile], kFlagPrefix | ((excl + block_total) & kValueMask));
-        s_excl = excl;
-      }
-    }
-  }
-  __syncthreads();
-  const unsigned long long incl = s_excl + incl_local;
-  if (idx < p.P) p.offsets[idx] = (uint32_t)incl;
-  const uint32_t last_tile = (uint32_t)((p.P + kScanBlock - 1) / kScanBlock) - 1u;
-  if (tile == last_tile && threadIdx.x == kScanBlock - 1) {
-    const unsigned long long total = s_excl + block_total;
-    p.hdr->num_rendered64 = total;
-    p.hdr->num_rendered = (uint32_t)(total > 0xffffffffull ? 0xffffffffull : total);
-    if (total > (unsigned long long)kMaxInstances) atomicOr(&p.hdr->status, kStatusOverflow);
+    for (int w = 0; w < kScanBlock / 32; ++w) total += s_warp[w];
+    if (total) atomicAdd(&p.hdr->num_rendered64, total);
   }
 }
 
@@ -212,7 +142,7 @@ __global__ void __launch_bounds__(kScanBlock) preprocess_scan_kernel(PreprocessP
 void launch_preprocess(const PreprocessParams& p, cudaStream_t s) {
   if (p.P <= 0) return;
   const int blocks = (p.P + kScanBlock - 1) / kScanBlock;
-  preprocess_scan_kernel<<<blocks, kScanBlock, 0, s>>>(p);
+  preprocess_kernel<<<blocks, kScanBlock, 0, s>>>(p);
 }
 
 }  // namespace omnigs

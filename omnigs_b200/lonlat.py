@@ -186,15 +186,21 @@ class LonlatState:
                     cull_extent=splat[:, 6:8], rgb=color[:, :3],
                     clamp_bits=color[:, 3].view(torch.int32),
                     depths=_view_tensor(self.geom, v.depth, P, torch.float32),
-                    offsets=_view_tensor(self.geom, v.offsets, P, torch.int32))
+                    tiles_touched=_view_tensor(self.geom, v.tiles_touched, P, torch.int32),
+                    depth_order=_view_tensor(self.geom, v.depth_order, P, torch.int32))
 
     def binning_view(self, num_rendered: int) -> dict:
+        """Sorted tile ids and point list; ``keys`` rebuilds the reference's 64-bit
+        ``tile << 32 | depth_bits`` keys from them."""
         v = capi.BinningView()
         capi.check(capi.lib().omnigs_lonlat_binning_view(self.binning.data_ptr(), self.binning.numel(),
                                                          self.W, self.H, ctypes.byref(v)),
                    "binning_view")
-        return dict(keys=_view_tensor(self.binning, v.keys, num_rendered, torch.int64),
-                    point_list=_view_tensor(self.binning, v.point_list, num_rendered, torch.int32))
+        tiles = _view_tensor(self.binning, v.tile_ids, num_rendered, torch.int32)
+        point_list = _view_tensor(self.binning, v.point_list, num_rendered, torch.int32)
+        depth_bits = self.geom_view()["depths"].view(torch.int32)[point_list.long()].to(torch.int64)
+        keys = (tiles.to(torch.int64) << 32) | (depth_bits & 0xFFFFFFFF)
+        return dict(tile_ids=tiles, point_list=point_list, keys=keys)
 
     def image_view(self) -> dict:
         v = capi.ImageView()

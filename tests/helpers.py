@@ -31,11 +31,6 @@ def run_cuda(g: lonlat.GaussianTensors, cam: lonlat.Camera, dpix: torch.Tensor |
     return out
 
 
-def tiles_touched(offsets: np.ndarray) -> np.ndarray:
-    o = offsets.astype(np.int64)
-    return np.diff(np.concatenate([[0], o])).astype(np.uint32)
-
-
 def oracle_stagewise(cu: dict, g_np: scenes.Gaussians, view: scenes.View, dpix_np, bg,
                      D=3, scale_modifier=1.0):
     """Oracle stages fed with the CUDA path's float intermediates."""
@@ -43,7 +38,7 @@ def oracle_stagewise(cu: dict, g_np: scenes.Gaussians, view: scenes.View, dpix_n
     radii = to_np(cu["radii"])
     means2D = to_np(cu["means2D"]).astype(np.float32)
     depths = to_np(cu["depths"]).astype(np.float32)
-    tt = tiles_touched(to_np(cu["offsets"]))
+    tt = to_np(cu["tiles_touched"]).view(np.uint32)
     b = oracle.binning(W, H, radii, means2D, depths, tt, f32=True)
     point_list = to_np(cu["point_list"]).astype(np.uint32)
     ranges = to_np(cu["ranges"]).astype(np.uint32)

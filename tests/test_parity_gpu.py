@@ -34,7 +34,7 @@ def test_preprocess_matches_fp64_oracle(cuda):
     vis = (radii > 0) & (pre["radii"] > 0)
     # integer outputs may differ from FP64 only where a value sits on a ceil/truncation boundary
     assert (radii != pre["radii"]).mean() < 2e-3
-    assert (helpers.tiles_touched(helpers.to_np(cu["offsets"])) != pre["tiles_touched"]).mean() < 2e-3
+    assert (helpers.to_np(cu["tiles_touched"]).view(np.uint32) != pre["tiles_touched"]).mean() < 2e-3
     lat = np.degrees(np.arcsin(np.abs(g.means3D[:, 1]) / np.linalg.norm(g.means3D, axis=1)))
     ok = vis & (lat < 80)
     np.testing.assert_allclose(helpers.to_np(cu["means2D"])[ok], pre["means2D"][ok], atol=2e-3, rtol=0)
@@ -192,7 +192,7 @@ def test_full_size_properties(cuda):
     dpix = torch.from_numpy(scenes.upstream_grad(W, H)).cuda()
     cu = helpers.run_cuda(gt, cam, dpix)
     n = cu["num_rendered"]
-    tt = helpers.tiles_touched(helpers.to_np(cu["offsets"]))
+    tt = helpers.to_np(cu["tiles_touched"]).view(np.uint32).astype(np.int64)
     assert n == int(tt.sum()) and n > 1_000_000
     keys = helpers.to_np(cu["keys"]).view(np.uint64)
     assert np.all(keys[1:] >= keys[:-1])
@@ -216,3 +216,40 @@ def test_full_size_properties(cuda):
     o = helpers.oracle_stagewise(cu, g, v, None, np.zeros(3, np.float32))
     err = np.abs(helpers.to_np(cu["image"]) - o["forward"]["image"])
     assert np.quantile(err, 0.9999) <= IMG_ATOL and err.max() <= 1e-3, (np.quantile(err, 0.9999), err.max())
+
+
+@pytest.mark.parametrize("clustered", [False, True])
+def test_binning_is_bit_exact_with_long_tiles(cuda, clustered):
+    """A tight cluster of splats puts more than 4096 instances in single tiles (and many equal
+    depths are impossible to order except by index); binning stays bit-exact."""
+    W, H = 512, 256
+    g = scenes.make_gaussians(6000, seed=12)
+    if clustered:
+        rng = np.random.default_rng(12)
+        d = np.array([0.0, 0.0, 1.0]) + 0.004 * rng.standard_normal((g.P, 3))
+        d /= np.linalg.norm(d, axis=1, keepdims=True)
+        g.means3D[:] = (d * np.linalg.norm(g.means3D, axis=1, keepdims=True)).astype(np.float32)
+        src = g.means3D[1::7].copy()
+        g.means3D[0:7 * len(src):7] = src  # duplicated positions: equal depths
+    v = scenes.identity_view(W, H)
+    gt, cam = lonlat.GaussianTensors.from_numpy(g), lonlat.Camera.from_view(v)
+    dpix = scenes.upstream_grad(W, H, seed=12)
+    cu = helpers.run_cuda(gt, cam, torch.from_numpy(dpix).cuda())
+    r = helpers.to_np(cu["ranges"]).astype(np.int64)
+    longest = int((r[:, 1] - r[:, 0]).max())
+    assert (longest > 4096) == clustered
+    o = helpers.oracle_stagewise(cu, g, v, dpix, np.zeros(3, np.float32))
+    np.testing.assert_array_equal(helpers.to_np(cu["keys"]).view(np.uint64), o["binning"]["keys"])
+    np.testing.assert_array_equal(helpers.to_np(cu["point_list"]).view(np.uint32), o["binning"]["point_list"])
+    np.testing.assert_array_equal(r.astype(np.uint32), o["binning"]["ranges"])
+    assert np.abs(helpers.to_np(cu["image"]) - o["forward"]["image"]).max() <= IMG_ATOL
+
+
+def test_depth_order_is_a_stable_sort_by_depth_bits(cuda):
+    g = scenes.make_gaussians(50_000, seed=13)
+    g.means3D[1::3] = g.means3D[0::3][: len(g.means3D[1::3])]  # many exactly equal depths
+    gt, cam = lonlat.GaussianTensors.from_numpy(g), lonlat.Camera.from_view(scenes.identity_view(256, 128))
+    cu = helpers.run_cuda(gt, cam)
+    bits = helpers.to_np(cu["depths"]).view(np.uint32)
+    want = np.argsort(bits, kind="stable").astype(np.int32)
+    np.testing.assert_array_equal(helpers.to_np(cu["depth_order"]), want)

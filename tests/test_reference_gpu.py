@@ -36,7 +36,9 @@ def _compare(P, W, H, seed, view=None, bg=(0.0, 0.0, 0.0), pole_fraction=0.0):
     # ---- integer stages: bit-exact ----
     torch.testing.assert_close(cu["radii"], r_radii, rtol=0, atol=0)
     assert cu["num_rendered"] == r_n
-    torch.testing.assert_close(cu["offsets"], rs["point_offsets"], rtol=0, atol=0)
+    torch.testing.assert_close(cu["tiles_touched"], rs["tiles_touched"], rtol=0, atol=0)
+    torch.testing.assert_close(torch.cumsum(cu["tiles_touched"].to(torch.int64), 0).to(torch.int32),
+                               rs["point_offsets"], rtol=0, atol=0)
     torch.testing.assert_close(cu["keys"], rs["keys"], rtol=0, atol=0)
     torch.testing.assert_close(cu["point_list"], rs["point_list"], rtol=0, atol=0)
     torch.testing.assert_close(cu["ranges"], rs["ranges"], rtol=0, atol=0)
