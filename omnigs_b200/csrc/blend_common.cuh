@@ -1,0 +1,89 @@
+// Shared pieces of the forward and backward tile blends: the pixel patch a warp owns, the
+// alpha-support box test against it, and the staging of a batch of splats into shared memory.
+#pragma once
+
+#include "device_util.cuh"
+#include "kernels.h"
+
+namespace omnigs {
+
+// Splats staged per shared-memory batch.
+constexpr int kBatch = 256;
+// Pixels per thread: a thread owns kBlendPx pixels of one column, 4 rows apart, so a warp (8
+// columns x 4 rows of threads) owns an 8 x (4 kBlendPx) patch and a block of kBlendThreads
+// threads one 16x16 tile.
+#ifndef OMNIGS_BLEND_PX
+#define OMNIGS_BLEND_PX 2
+#endif
+constexpr int kBlendPx = OMNIGS_BLEND_PX;
+static_assert(kBlendPx == 1 || kBlendPx == 2 || kBlendPx == 4, "a 16x16 tile splits into 8/kBlendPx warps");
+constexpr int kBlendThreads = 256 / kBlendPx;
+constexpr int kBlendWarps = kBlendThreads / 32;
+
+struct BlendPatch {
+  int px, py0;       // this thread's column and first row
+  float pxf;         // column as float
+  float wcx, wcy;    // centre of the warp's patch
+
+  static __device__ __forceinline__ BlendPatch make() {
+    const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
+    const int wx0 = blockIdx.x * 16 + (warp & 1) * 8;
+    const int wy0 = blockIdx.y * 16 + (warp >> 1) * 4 * kBlendPx;
+    BlendPatch b;
+    b.px = wx0 + (lane & 7);
+    b.py0 = wy0 + (lane >> 3);
+    b.pxf = (float)b.px;
+    b.wcx = (float)wx0 + 3.5f;
+    b.wcy = (float)wy0 + 0.5f * (4 * kBlendPx - 1);
+    return b;
+  }
+  __device__ __forceinline__ int py(int i) const { return py0 + 4 * i; }
+  __device__ __forceinline__ float pyf(int i) const { return (float)(py0 + 4 * i); }
+  __device__ __forceinline__ bool inside(int i, int W, int H) const { return px < W && py(i) < H; }
+  __device__ __forceinline__ int64_t pixel(int i, int W) const { return (int64_t)py(i) * W + px; }
+  // The splat's alpha-support box (centre a.xy, half extents b.zw) touches the patch.  Written as
+  // a negated "misses" test so that NaN extents count as touching (the per-pixel test decides).
+  __device__ __forceinline__ bool hit(const float4& a, const float4& b) const {
+    return !(fabsf(a.x - wcx) > b.z + 3.5f || fabsf(a.y - wcy) > b.w + (2.0f * kBlendPx - 0.5f));
+  }
+};
+
+// Exponent of the splat's Gaussian at offset d = centre - pixel (forward.cu:416, backward.cu:763):
+//   power = -0.5 (ca dx^2 + cc dy^2) - cb dx dy.
+// The reference leaves the rounding of this expression to the compiler's FMA contraction.  It is
+// written here with explicit roundings in the one fusion that reproduces the reference's compiled
+// results bit for bit (checked on the 1M-Gaussian 2048x1024 scene: identical transmittance, last
+// contributors and image): ca dx dx fused into the sum with the rounded cc dy dy, the cb dx dy term
+// rounded on its own.  Being explicit keeps the result independent of how the surrounding kernel is
+// structured (a thread owning several pixels lets the compiler share products between them and
+// choose other fusions).  The forward and backward use the same function, so they agree on every
+// 1/255 and saturation decision.
+__device__ __forceinline__ float splat_power(const float4& a, const float4& b, float2 d) {
+  const float ca_dx = __fmul_rn(a.z, d.x), cc_dy = __fmul_rn(b.x, d.y), cb_dx = __fmul_rn(a.w, d.x);
+  const float quad = __fmaf_rn(ca_dx, d.x, __fmul_rn(cc_dy, d.y));
+  return __fsub_rn(__fmul_rn(-0.5f, quad), __fmul_rn(cb_dx, d.y));
+}
+
+// Stages instances [base, base + cnt) of the tile's list (from the back when reverse: slot t holds
+// position base_hi - 1 - t, with base the exclusive upper end) into shared memory.
+__device__ __forceinline__ void stage_batch(const RenderParams& p, uint32_t range_begin, int base, int cnt,
+                                            bool reverse, float4* s_a, float4* s_b, float4* s_c,
+                                            uint32_t* s_g) {
+  for (int t = threadIdx.x; t < cnt; t += kBlendThreads) {
+    const uint32_t pos = reverse ? (uint32_t)(base - 1 - t) : (uint32_t)(base + t);
+    const uint32_t g = p.point_list[range_begin + pos];
+    if (g < (uint32_t)p.P) {
+      if (s_g) s_g[t] = g;
+      s_a[t] = p.splat[2 * g];
+      s_b[t] = p.splat[2 * g + 1];
+      s_c[t] = p.color[g];
+    } else {  // unreachable for a consistent instance list; stage a splat that never contributes
+      if (s_g) s_g[t] = 0;
+      s_a[t] = make_float4(__int_as_float(0x7f800000), 0.f, 0.f, 0.f);
+      s_b[t] = make_float4(0.f, 0.f, -__int_as_float(0x7f800000), -__int_as_float(0x7f800000));
+      s_c[t] = make_float4(0.f, 0.f, 0.f, 0.f);
+    }
+  }
+}
+
+}  // namespace omnigs

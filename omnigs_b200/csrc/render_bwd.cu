@@ -1,21 +1,20 @@
 // Backward back-to-front blend of one 16x16 tile per block (backward.cu:672-843).
 //
-// Per pixel this replays the reference's recurrence exactly: start from the stored final
-// transmittance and last-contributor index, walk the tile's instances from the back, undo
-// T /= (1 - alpha) and accumulate the colour-behind term.  The per-(pixel, splat) gradients
-// (2 screen-space mean, 3 conic, 1 opacity, 3 colour) are not pushed with 9 global atomics per
-// pixel as in the reference: the warp that owns an 8x4 pixel patch reduces them first, with a
-// reduce-scatter of 8 values (9 shuffles) plus a butterfly for the ninth, and then 8 lanes add one
-// 32-byte accumulator record per splat.  Warps skip splats whose alpha-support box misses their
-// patch or that lie behind all of their pixels' last contributors, and the block starts at the
-// batch holding its largest last contributor instead of at the end of the range.
-#include "device_util.cuh"
-#include "kernels.h"
+// Per pixel this replays the reference's recurrence: start from the stored final transmittance
+// and last-contributor index, walk the tile's instances from the back, undo T /= (1 - alpha) and
+// accumulate the colour-behind term.  (One correctly rounded reciprocal of 1 - alpha serves both
+// of the reference's divisions by it.)  The per-(pixel, splat) gradients (2 screen-space mean, 3
+// conic, 1 opacity, 3 colour) are not pushed with 9 global atomics per pixel as in the reference:
+// a thread first sums them over its kBlendPx pixels, the warp that owns the 8 x (4 kBlendPx) patch
+// reduces them with a reduce-scatter of 8 values (9 shuffles) plus a butterfly for the ninth, and
+// 8 lanes add one accumulator record per splat; when a single lane contributes it adds its 9
+// values directly.  Warps skip splats whose alpha-support box misses their patch or that lie
+// behind all of their pixels' last contributors, and the block starts at the batch holding its
+// largest last contributor instead of at the end of the range.
+#include "blend_common.cuh"
 
 namespace omnigs {
 namespace {
-
-constexpr int kBatch = 256;
 
 // Sums v[0..8] over the warp and adds the totals to acc[0..8] (one accumulator record).
 __device__ __forceinline__ void warp_reduce_add9(const float v[9], float* acc, int lane) {
@@ -50,128 +49,132 @@ __device__ __forceinline__ void warp_reduce_add9(const float v[9], float* acc, i
   if (lane == 0) atomicAdd(acc + 8, e);
 }
 
-__global__ void __launch_bounds__(256) render_backward_kernel(RenderParams p) {
+struct PixelState {
+  float T, T_final;
+  uint32_t last_contributor;
+  float dpix[3];
+  float bg_dot_dpixel;
+  float accum_rec[3];
+  float last_color[3];
+  float last_alpha;
+};
+
+__global__ void __launch_bounds__(kBlendThreads) render_backward_kernel(RenderParams p) {
   __shared__ float4 s_a[kBatch];
   __shared__ float4 s_b[kBatch];
   __shared__ float4 s_c[kBatch];
   __shared__ uint32_t s_g[kBatch];
-  __shared__ uint32_t s_warp_last[8];
+  __shared__ uint32_t s_warp_last[kBlendWarps];
+  const BlendPatch patch = BlendPatch::make();
   const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
-  const int wx0 = blockIdx.x * 16 + (warp & 1) * 8;
-  const int wy0 = blockIdx.y * 16 + (warp >> 1) * 4;
-  const int px = wx0 + (lane & 7), py = wy0 + (lane >> 3);
-  const bool inside = px < p.W && py < p.H;
-  const float2 pixf = {(float)px, (float)py};
-  const float wcx = (float)wx0 + 3.5f, wcy = (float)wy0 + 1.5f;
 
   uint2 range = p.ranges[blockIdx.y * p.gx + blockIdx.x];
   if (range.y > (uint64_t)p.capacity || range.x > range.y) range = make_uint2(0, 0);
   const uint32_t n = range.y - range.x;
 
-  const int64_t pix = (int64_t)py * p.W + px;
   const int64_t HW = (int64_t)p.H * p.W;
-  const float T_final = inside ? p.final_T[pix] : 0.f;
-  float T = T_final;
-  uint32_t last_contributor = inside ? p.n_contrib[pix] : 0u;
-  if (last_contributor > n) last_contributor = n;
-  float dpix[3] = {0.f, 0.f, 0.f};
-  if (inside) {
-    dpix[0] = p.dL_dpix[pix];
-    dpix[1] = p.dL_dpix[HW + pix];
-    dpix[2] = p.dL_dpix[2 * HW + pix];
-  }
-  float bg_dot_dpixel = 0;
+  PixelState ps[kBlendPx];
+  uint32_t thread_last = 0;
 #pragma unroll
-  for (int i = 0; i < 3; i++) bg_dot_dpixel += p.bg[i] * dpix[i];
+  for (int i = 0; i < kBlendPx; ++i) {
+    PixelState& s = ps[i];
+    const bool in = patch.inside(i, p.W, p.H);
+    const int64_t pix = in ? patch.pixel(i, p.W) : 0;
+    s.T_final = in ? p.final_T[pix] : 0.f;
+    s.T = s.T_final;
+    s.last_contributor = in ? p.n_contrib[pix] : 0u;
+    if (s.last_contributor > n) s.last_contributor = n;
+    thread_last = max(thread_last, s.last_contributor);
+    s.dpix[0] = in ? p.dL_dpix[pix] : 0.f;
+    s.dpix[1] = in ? p.dL_dpix[HW + pix] : 0.f;
+    s.dpix[2] = in ? p.dL_dpix[2 * HW + pix] : 0.f;
+    s.bg_dot_dpixel = 0.f;
+#pragma unroll
+    for (int ch = 0; ch < 3; ch++) s.bg_dot_dpixel += p.bg[ch] * s.dpix[ch];
+    s.accum_rec[0] = s.accum_rec[1] = s.accum_rec[2] = 0.f;
+    s.last_color[0] = s.last_color[1] = s.last_color[2] = 0.f;
+    s.last_alpha = 0.f;
+  }
   const float ddelx_dx = 0.5 * p.W;
   const float ddely_dy = 0.5 * p.H;
-  float accum_rec[3] = {0.f, 0.f, 0.f};
-  float last_color[3] = {0.f, 0.f, 0.f};
-  float last_alpha = 0.f;
 
-  const uint32_t warp_last = __reduce_max_sync(kFullMask, last_contributor);
+  const uint32_t warp_last = __reduce_max_sync(kFullMask, thread_last);
   if (lane == 0) s_warp_last[warp] = warp_last;
   __syncthreads();
   uint32_t block_last = 0;
 #pragma unroll
-  for (int w = 0; w < 8; ++w) block_last = max(block_last, s_warp_last[w]);
+  for (int w = 0; w < kBlendWarps; ++w) block_last = max(block_last, s_warp_last[w]);
 
   for (int hi = (int)block_last; hi > 0; hi -= kBatch) {
     const int cnt = min(kBatch, hi);
     __syncthreads();
-    if ((int)threadIdx.x < cnt) {
-      const uint32_t pos = (uint32_t)(hi - 1 - (int)threadIdx.x);
-      const uint32_t g = p.point_list[range.x + pos];
-      if (g < (uint32_t)p.P) {
-        s_g[threadIdx.x] = g;
-        s_a[threadIdx.x] = p.splat[2 * g];
-        s_b[threadIdx.x] = p.splat[2 * g + 1];
-        s_c[threadIdx.x] = p.color[g];
-      } else {  // unreachable for a consistent instance list; stage a splat that never contributes
-        s_g[threadIdx.x] = 0;
-        s_a[threadIdx.x] = make_float4(__int_as_float(0x7f800000), 0.f, 0.f, 0.f);
-        s_b[threadIdx.x] = make_float4(0.f, 0.f, -__int_as_float(0x7f800000), -__int_as_float(0x7f800000));
-        s_c[threadIdx.x] = make_float4(0.f, 0.f, 0.f, 0.f);
-      }
-    }
+    stage_batch(p, range.x, hi, cnt, /*reverse=*/true, s_a, s_b, s_c, s_g);
     __syncthreads();
     for (int k = 0; k * 32 < cnt; ++k) {
       const int j = k * 32 + lane;
       bool hit = false;
-      if (j < cnt && (uint32_t)(hi - 1 - j) < warp_last) {
-        const float4 a = s_a[j];
-        const float4 b = s_b[j];
-        hit = !(fabsf(a.x - wcx) > b.z + 3.5f || fabsf(a.y - wcy) > b.w + 1.5f);
-      }
+      if (j < cnt && (uint32_t)(hi - 1 - j) < warp_last) hit = patch.hit(s_a[j], s_b[j]);
       unsigned m = __ballot_sync(kFullMask, hit);
       while (m) {
         const int jj = k * 32 + __ffs(m) - 1;
         m &= m - 1;
         const uint32_t pos = (uint32_t)(hi - 1 - jj);
+        const float4 a = s_a[jj];
+        const float4 b = s_b[jj];
         float v[9] = {0.f, 0.f, 0.f, 0.f, 0.f, 0.f, 0.f, 0.f, 0.f};
         bool contrib = false;
-        if (pos < last_contributor) {
-          const float4 a = s_a[jj];
-          const float4 b = s_b[jj];
-          const float2 d = {a.x - pixf.x, a.y - pixf.y};
-          const float power = -0.5f * (a.z * d.x * d.x + b.x * d.y * d.y) - a.w * d.x * d.y;
-          if (!(power > 0.0f)) {
-            const float G = expf(power);
-            const float alpha = fminf(0.99f, b.y * G);
-            if (!(alpha < 1.0f / 255.0f)) {
-              contrib = true;
-              T = T / (1.f - alpha);
-              const float dchannel_dcolor = alpha * T;
-              const float4 cv = s_c[jj];
-              const float col[3] = {cv.x, cv.y, cv.z};
-              float dL_dalpha = 0.0f;
 #pragma unroll
-              for (int ch = 0; ch < 3; ch++) {
-                const float c = col[ch];
-                accum_rec[ch] = last_alpha * last_color[ch] + (1.f - last_alpha) * accum_rec[ch];
-                last_color[ch] = c;
-                const float dL_dchannel = dpix[ch];
-                dL_dalpha += (c - accum_rec[ch]) * dL_dchannel;
-                v[6 + ch] = dchannel_dcolor * dL_dchannel;
-              }
-              dL_dalpha *= T;
-              last_alpha = alpha;
-              dL_dalpha += (-T_final / (1.f - alpha)) * bg_dot_dpixel;
-              const float dL_dG = b.y * dL_dalpha;
-              const float gdx = G * d.x;
-              const float gdy = G * d.y;
-              const float dG_ddelx = -gdx * a.z - gdy * a.w;
-              const float dG_ddely = -gdy * b.x - gdx * a.w;
-              v[0] = dL_dG * dG_ddelx * ddelx_dx;
-              v[1] = dL_dG * dG_ddely * ddely_dy;
-              v[2] = -0.5f * gdx * d.x * dL_dG;
-              v[3] = -0.5f * gdx * d.y * dL_dG;
-              v[4] = -0.5f * gdy * d.y * dL_dG;
-              v[5] = G * dL_dalpha;
-            }
+        for (int i = 0; i < kBlendPx; ++i) {
+          PixelState& s = ps[i];
+          if (pos >= s.last_contributor) continue;
+          const float2 d = {a.x - patch.pxf, a.y - patch.pyf(i)};
+          const float power = splat_power(a, b, d);
+          if (power > 0.0f) continue;
+          const float G = expf(power);
+          const float alpha = fminf(0.99f, b.y * G);
+          if (alpha < 1.0f / 255.0f) continue;
+          contrib = true;
+          const float inv_one_minus_alpha = __frcp_rn(1.f - alpha);
+          s.T = s.T * inv_one_minus_alpha;
+          const float dchannel_dcolor = alpha * s.T;
+          const float4 cv = s_c[jj];
+          const float col[3] = {cv.x, cv.y, cv.z};
+          float dL_dalpha = 0.0f;
+#pragma unroll
+          for (int ch = 0; ch < 3; ch++) {
+            const float c = col[ch];
+            s.accum_rec[ch] = s.last_alpha * s.last_color[ch] + (1.f - s.last_alpha) * s.accum_rec[ch];
+            s.last_color[ch] = c;
+            const float dL_dchannel = s.dpix[ch];
+            dL_dalpha += (c - s.accum_rec[ch]) * dL_dchannel;
+            v[6 + ch] += dchannel_dcolor * dL_dchannel;
           }
+          dL_dalpha *= s.T;
+          s.last_alpha = alpha;
+          dL_dalpha += (-s.T_final * inv_one_minus_alpha) * s.bg_dot_dpixel;
+          const float dL_dG = b.y * dL_dalpha;
+          const float gdx = G * d.x;
+          const float gdy = G * d.y;
+          const float dG_ddelx = -gdx * a.z - gdy * a.w;
+          const float dG_ddely = -gdy * b.x - gdx * a.w;
+          v[0] += dL_dG * dG_ddelx * ddelx_dx;
+          v[1] += dL_dG * dG_ddely * ddely_dy;
+          v[2] += -0.5f * gdx * d.x * dL_dG;
+          v[3] += -0.5f * gdx * d.y * dL_dG;
+          v[4] += -0.5f * gdy * d.y * dL_dG;
+          v[5] += G * dL_dalpha;
         }
-        if (__any_sync(kFullMask, contrib)) warp_reduce_add9(v, p.grad_acc + 12 * (size_t)s_g[jj], lane);
+        const unsigned cm = __ballot_sync(kFullMask, contrib);
+        if (cm == 0) continue;
+        float* acc = p.grad_acc + 12 * (size_t)s_g[jj];
+        if ((cm & (cm - 1)) == 0) {  // one contributing lane: add its values directly
+          if (contrib) {
+#pragma unroll
+            for (int q = 0; q < 9; ++q) atomicAdd(acc + q, v[q]);
+          }
+        } else {
+          warp_reduce_add9(v, acc, lane);
+        }
       }
     }
   }
@@ -181,7 +184,7 @@ __global__ void __launch_bounds__(256) render_backward_kernel(RenderParams p) {
 
 void launch_render_backward(const RenderParams& p, cudaStream_t s) {
   if (p.gx <= 0 || p.gy <= 0) return;
-  render_backward_kernel<<<dim3(p.gx, p.gy), 256, 0, s>>>(p);
+  render_backward_kernel<<<dim3(p.gx, p.gy), kBlendThreads, 0, s>>>(p);
 }
 
 }  // namespace omnigs
