@@ -162,6 +162,114 @@ int omnigs_lonlat_backward(const OmnigsLonlatBackwardArgs* args, void* geom, siz
                            const void* binning, size_t binning_bytes, const void* image,
                            size_t image_bytes, omnigs_stream_t stream);
 
+/* ---------------------------------------------------------------- batched views -------------
+ * Many equirect views of uneven resolution over one shared Gaussian set, rendered and
+ * back-propagated with one launch per stage for the whole batch.  The reference renders one view
+ * per call (GaussianRenderer::renderLonlat, src/gaussian_renderer.cpp:167, driven per keyframe by
+ * GaussianMapper::trainForOneIteration, src/gaussian_mapper.cpp:290-440); a batch of V views
+ * produces per view exactly the image of a single-view forward (same sorted instance lists, same
+ * per-pixel arithmetic) and gradients equal to the sum of the V single-view backwards, summed on
+ * the device instead of by V separate kernels.  The backward also accumulates the trainer's
+ * densification statistics (gaussian_mapper.cpp:423-428, gaussian_model.cpp:839-853).
+ *
+ * State: one caller-owned buffer of omnigs_batch_state_bytes() for the per-(view, Gaussian)
+ * records and per-pixel state, plus a binning buffer of omnigs_lonlat_binning_bytes(capacity) for
+ * the instances of all views together.  Nothing synchronises the host except
+ * omnigs_batch_read_status; a batch whose instances exceed the capacity sets
+ * OMNIGS_STATUS_CAPACITY, skips binning and blending, and can be resumed with omnigs_batch_render
+ * after the binning buffer is grown.  The per-view pose arrays are read on the device when the
+ * kernels run, so a captured CUDA graph of these calls replays with updated poses.
+ *
+ * Precision options: sh_dtype OMNIGS_SH_BF16 reads SH coefficients stored as bfloat16 (colour,
+ * transmittance and all gradients still accumulate in FP32; dL_dsh is FP32); fp64_poles evaluates
+ * the 2D covariance, its inverse and its backward in FP64 for Gaussians beyond 85 degrees of
+ * latitude in a view, where the lonlat Jacobian degenerates.  With both off, every view's image
+ * and instance list are bit-identical to omnigs_lonlat_forward's. */
+#define OMNIGS_MAX_BATCH_VIEWS 32
+#define OMNIGS_SH_FP32 0
+#define OMNIGS_SH_BF16 1
+
+typedef struct OmnigsBatchView {
+  int W, H;
+  float* out_color;            /* [3,H,W] output of the forward */
+  const float* dL_dout_color;  /* [3,H,W] input of the backward (unused by the forward) */
+} OmnigsBatchView;
+
+typedef struct OmnigsBatchArgs {
+  int P, D, M;                 /* Gaussians, active SH degree, SH coefficients per Gaussian */
+  int V;                       /* views, 1..OMNIGS_MAX_BATCH_VIEWS */
+  int sh_dtype;                /* OMNIGS_SH_FP32 or OMNIGS_SH_BF16 */
+  int fp64_poles;              /* 0 or 1 */
+  const float* means3D;        /* [P,3] */
+  const void* shs;             /* [P,M,3] fp32 or bf16, or NULL (then colors_precomp) */
+  const float* colors_precomp; /* [P,3] or NULL */
+  const float* opacities;      /* [P] */
+  const float* scales;         /* [P,3] or NULL (then cov3D_precomp) */
+  float scale_modifier;
+  const float* rotations;      /* [P,4] or NULL */
+  const float* cov3D_precomp;  /* [P,6] or NULL */
+  const float* viewmatrices;   /* [V,16] device, each Tcw column-major as in the single-view args */
+  const float* campos;         /* [V,3] device */
+  const float* backgrounds;    /* [V,3] device */
+  const OmnigsBatchView* views;/* [V] host array */
+} OmnigsBatchArgs;
+
+/* Gradient outputs of the batched backward: parameter gradients summed over the views (fully
+ * written), plus optional densification statistics accumulated in place over the views where
+ * the Gaussian is visible (radius > 0): grad_accum += |dL/dmean2D.xy| (viewspace-point gradient,
+ * NDC scale), denom += 1, max_radii = max(max_radii, radius). */
+typedef struct OmnigsBatchGrads {
+  float* dL_dmeans3D;   /* [P,3] */
+  float* dL_dsh;        /* [P,M,3] fp32, or NULL without SH */
+  float* dL_dopacity;   /* [P] */
+  float* dL_dscales;    /* [P,3] */
+  float* dL_drotations; /* [P,4] */
+  float* dL_dcolors;    /* [P,3] or NULL */
+  float* dL_dcov3D;     /* [P,6] or NULL */
+  float* grad_accum;    /* [P] or NULL */
+  float* denom;         /* [P] or NULL */
+  float* max_radii;     /* [P] or NULL */
+} OmnigsBatchGrads;
+
+/* Size of the batch state buffer for P Gaussians and V views of sizes W[v] x H[v] (0 if the
+ * arguments are invalid). */
+size_t omnigs_batch_state_bytes(int P, int V, const int* W, const int* H);
+
+/* Preprocess of every view, then omnigs_batch_render. */
+int omnigs_batch_forward(const OmnigsBatchArgs* args, void* state, size_t state_bytes, void* binning,
+                         size_t binning_bytes, omnigs_stream_t stream);
+
+/* Binning and forward blend of all views from a state filled by a preprocess (resume after a
+ * capacity overflow). */
+int omnigs_batch_render(const OmnigsBatchArgs* args, void* state, size_t state_bytes, void* binning,
+                        size_t binning_bytes, omnigs_stream_t stream);
+
+/* Backward blend of all views and the batched backward preprocess. */
+int omnigs_batch_backward(const OmnigsBatchArgs* args, const OmnigsBatchGrads* grads, void* state,
+                          size_t state_bytes, const void* binning, size_t binning_bytes,
+                          omnigs_stream_t stream);
+
+/* Waits for `stream`; returns the total instance count, the per-view counts (view_rendered[V], may
+ * be NULL) and the status word. */
+int omnigs_batch_read_status(const void* state, int V, int64_t* num_rendered, int64_t* view_rendered,
+                             uint32_t* status, omnigs_stream_t stream);
+
+/* Device pointers into the batch state, for inspection and parity testing.  Pixels of view v start
+ * at pixel_base[v] of final_T / n_contrib, its tiles at tile_base[v] of ranges. */
+typedef struct OmnigsBatchStateView {
+  const int* radii;             /* [V][P] */
+  const float* splat;           /* [V][P][8] */
+  const float* color;           /* [V][P][4] */
+  const float* final_T;         /* [pixels] */
+  const uint32_t* n_contrib;    /* [pixels] */
+  const uint32_t* ranges;       /* [tiles][2] */
+  int64_t pixel_base[OMNIGS_MAX_BATCH_VIEWS];
+  int64_t tile_base[OMNIGS_MAX_BATCH_VIEWS];
+  int tile_passes;              /* tile-sort passes: the sorted list is in buffer (tile_passes & 1) */
+} OmnigsBatchStateView;
+int omnigs_batch_state_view(const void* state, int P, int V, const int* W, const int* H,
+                            OmnigsBatchStateView* out);
+
 /* Visibility marks.  camera_type 3: every Gaussian (markAllVisible, rasterizer_impl.cu:82-90);
  * camera_type 1: the pinhole near test p_view.z > 0.2 (checkFrustum, rasterizer_impl.cu:66-78,
  * auxiliary.h:166-196).  present is a [P] byte array. */

@@ -67,6 +67,36 @@ class ImageView(ctypes.Structure):
     _fields_ = [("final_T", _vp), ("n_contrib", _vp), ("ranges", _vp)]
 
 
+MAX_BATCH_VIEWS = 32
+SH_FP32 = 0
+SH_BF16 = 1
+
+
+class BatchView(ctypes.Structure):
+    _fields_ = [("W", _i), ("H", _i), ("out_color", _vp), ("dL_dout_color", _vp)]
+
+
+class BatchArgs(ctypes.Structure):
+    _fields_ = [("P", _i), ("D", _i), ("M", _i), ("V", _i), ("sh_dtype", _i), ("fp64_poles", _i),
+                ("means3D", _vp), ("shs", _vp), ("colors_precomp", _vp), ("opacities", _vp),
+                ("scales", _vp), ("scale_modifier", _f), ("rotations", _vp), ("cov3D_precomp", _vp),
+                ("viewmatrices", _vp), ("campos", _vp), ("backgrounds", _vp),
+                ("views", ctypes.POINTER(BatchView))]
+
+
+class BatchGrads(ctypes.Structure):
+    _fields_ = [("dL_dmeans3D", _vp), ("dL_dsh", _vp), ("dL_dopacity", _vp), ("dL_dscales", _vp),
+                ("dL_drotations", _vp), ("dL_dcolors", _vp), ("dL_dcov3D", _vp),
+                ("grad_accum", _vp), ("denom", _vp), ("max_radii", _vp)]
+
+
+class BatchStateView(ctypes.Structure):
+    _fields_ = [("radii", _vp), ("splat", _vp), ("color", _vp), ("final_T", _vp),
+                ("n_contrib", _vp), ("ranges", _vp),
+                ("pixel_base", ctypes.c_int64 * MAX_BATCH_VIEWS),
+                ("tile_base", ctypes.c_int64 * MAX_BATCH_VIEWS), ("tile_passes", _i)]
+
+
 # every symbol include/omnigs_b200.h declares
 EXPORTED = ["omnigs_version", "omnigs_last_error", "omnigs_lonlat_geom_bytes",
             "omnigs_lonlat_image_bytes", "omnigs_lonlat_binning_bytes",
@@ -75,7 +105,9 @@ EXPORTED = ["omnigs_version", "omnigs_last_error", "omnigs_lonlat_geom_bytes",
             "omnigs_lonlat_backward",
             "omnigs_mark_visible", "omnigs_timing_enable", "omnigs_timing_read",
             "omnigs_kernel_launches", "omnigs_lonlat_geom_view", "omnigs_lonlat_binning_view",
-            "omnigs_lonlat_image_view"]
+            "omnigs_lonlat_image_view", "omnigs_batch_state_bytes", "omnigs_batch_forward",
+            "omnigs_batch_render", "omnigs_batch_backward", "omnigs_batch_read_status",
+            "omnigs_batch_state_view"]
 
 _lib = None
 
@@ -114,6 +146,18 @@ def lib() -> ctypes.CDLL:
         L.omnigs_lonlat_binning_view.argtypes = [_vp, ctypes.c_size_t, _i, _i,
                                                  ctypes.POINTER(BinningView)]
         L.omnigs_lonlat_image_view.argtypes = [_vp, _i, _i, ctypes.POINTER(ImageView)]
+        ip = ctypes.POINTER(_i)
+        L.omnigs_batch_state_bytes.restype = ctypes.c_size_t
+        L.omnigs_batch_state_bytes.argtypes = [_i, _i, ip, ip]
+        bfw = [ctypes.POINTER(BatchArgs), _vp, ctypes.c_size_t, _vp, ctypes.c_size_t, _vp]
+        L.omnigs_batch_forward.argtypes = bfw
+        L.omnigs_batch_render.argtypes = bfw
+        L.omnigs_batch_backward.argtypes = [ctypes.POINTER(BatchArgs), ctypes.POINTER(BatchGrads), _vp,
+                                            ctypes.c_size_t, _vp, ctypes.c_size_t, _vp]
+        L.omnigs_batch_read_status.argtypes = [_vp, _i, ctypes.POINTER(ctypes.c_int64),
+                                               ctypes.POINTER(ctypes.c_int64),
+                                               ctypes.POINTER(ctypes.c_uint32), _vp]
+        L.omnigs_batch_state_view.argtypes = [_vp, _i, _i, ip, ip, ctypes.POINTER(BatchStateView)]
         _lib = L
     return _lib
 
@@ -154,6 +198,14 @@ def binning_bytes(capacity: int) -> int:
 
 def binning_capacity(nbytes: int) -> int:
     return int(lib().omnigs_lonlat_binning_capacity(nbytes))
+
+
+def batch_state_bytes(P: int, sizes) -> int:
+    """Bytes of the batch state for P Gaussians and views of the given (W, H) sizes (0 if invalid)."""
+    V = len(sizes)
+    W = (_i * max(V, 1))(*[w for w, _ in sizes])
+    H = (_i * max(V, 1))(*[h for _, h in sizes])
+    return int(lib().omnigs_batch_state_bytes(P, V, W, H))
 
 
 def timing_enable(on: bool):

@@ -49,14 +49,15 @@ __global__ void __launch_bounds__(256) histogram_kernel(HistParams p) {
   __shared__ uint32_t s_hist[kDepthPasses][kRadix];
   for (int i = threadIdx.x; i < kDepthPasses * kRadix; i += blockDim.x) (&s_hist[0][0])[i] = 0;
   __syncthreads();
-  const uint32_t n = item_count(p.count_hdr, p.n_host, p.capacity);
+  const uint32_t n = p.seg_len ? p.seg_len : item_count(p.count_hdr, p.n_host, p.capacity);
+  const size_t seg_base = (size_t)blockIdx.y * n;  // gridDim.y segments
   const int lane = threadIdx.x & 31;
   const uint32_t stride = gridDim.x * blockDim.x;
   // whole warps iterate together so that match.any sees all 32 lanes
   for (uint32_t base = blockIdx.x * blockDim.x + (threadIdx.x & ~31u); base < n; base += stride) {
     const uint32_t i = base + lane;
     const bool valid = i < n;
-    const uint32_t key = valid ? p.keys[i] : 0u;
+    const uint32_t key = valid ? p.keys[seg_base + i] : 0u;
     for (int q = 0; q < p.passes; ++q) {
       const uint32_t digit = (key >> p.shift[q]) & p.mask[q];
       const unsigned peers = __match_any_sync(kFullMask, valid ? digit : (0x10000u | lane));
@@ -64,9 +65,10 @@ __global__ void __launch_bounds__(256) histogram_kernel(HistParams p) {
     }
   }
   __syncthreads();
+  uint32_t* hist = p.hist + (size_t)blockIdx.y * p.passes * kRadix;
   for (int i = threadIdx.x; i < p.passes * kRadix; i += blockDim.x) {
     const uint32_t v = (&s_hist[0][0])[i];
-    if (v) atomicAdd(&p.hist[i], v);
+    if (v) atomicAdd(&hist[i], v);
   }
 }
 
@@ -113,16 +115,27 @@ __device__ __forceinline__ uint32_t block_exclusive_scan(uint32_t v, uint32_t* s
 // ranks a 4096-item tile in shared memory (warp multi-split with match.any: equal digits keep
 // their input order), publishes its per-digit counts, resolves its global digit offsets by
 // decoupled look-back (tiles are taken in launch order from an atomic counter, so a block only
-// waits on blocks that are already running) and writes runs of equal digits coalesced.
+// waits on blocks that are already running) and writes runs of equal digits coalesced.  In a
+// segmented sort every segment is an independent sort whose look-back chain starts at the
+// segment's first tile; a value-less first pass numbers items by their global index.
 __global__ void __launch_bounds__(kSortThreads, 3) onesweep_kernel(OnesweepParams p) {
   __shared__ SortSmem sm;
-  const uint32_t n = item_count(p.count_hdr, p.n_host, p.capacity);
-  const uint32_t ntiles = (n + kSortTile - 1) / kSortTile;
+  const uint32_t n = p.seg_len ? p.seg_len : item_count(p.count_hdr, p.n_host, p.capacity);
+  const uint32_t tiles_per_seg = (n + kSortTile - 1) / kSortTile;
+  const uint32_t ntiles = tiles_per_seg * (p.seg_len ? p.num_segs : 1u);
   if (threadIdx.x == 0) sm.tile = atomicAdd(p.tile_counter, 1u);
   for (int i = threadIdx.x; i < (kSortThreads / 32) * kRadix; i += kSortThreads) (&sm.warp_hist[0][0])[i] = 0;
   __syncthreads();
-  const uint32_t tile = sm.tile;
-  if (tile >= ntiles) return;
+  const uint32_t ticket = sm.tile;
+  if (ticket >= ntiles) return;
+  const uint32_t seg = ticket / tiles_per_seg;
+  const uint32_t tile = ticket - seg * tiles_per_seg;  // tile index within the segment
+  const size_t seg_base = (size_t)seg * n;
+  const uint32_t* keys_in = p.keys_in + seg_base;
+  const uint32_t* vals_in = p.vals_in ? p.vals_in + seg_base : nullptr;
+  uint32_t* keys_out = p.keys_out + seg_base;
+  uint32_t* vals_out = p.vals_out + seg_base;
+  const uint32_t* hist = p.hist + (size_t)seg * p.hist_seg_stride;
   const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
   const unsigned lt_mask = (1u << lane) - 1u;
   const uint32_t mask = p.mask;
@@ -134,16 +147,16 @@ __global__ void __launch_bounds__(kSortThreads, 3) onesweep_kernel(OnesweepParam
 #pragma unroll
   for (int k = 0; k < kSortItems; ++k) {
     const uint32_t idx = tile_base + k * 32;
-    key[k] = idx < n ? p.keys_in[idx] : 0xffffffffu;
+    key[k] = idx < n ? keys_in[idx] : 0xffffffffu;
   }
 #pragma unroll
   for (int k = 0; k < kSortItems; ++k) {
     const uint32_t idx = tile_base + k * 32;
-    val[k] = idx < n ? (p.vals_in ? p.vals_in[idx] : idx) : 0u;
+    val[k] = idx < n ? (vals_in ? vals_in[idx] : (uint32_t)(seg_base + idx)) : 0u;
   }
   // where each digit starts in the whole output
   uint32_t unused;
-  sm.global_base[threadIdx.x] = block_exclusive_scan(p.hist[threadIdx.x], sm.scan_tmp, unused);
+  sm.global_base[threadIdx.x] = block_exclusive_scan(hist[threadIdx.x], sm.scan_tmp, unused);
 
   uint32_t rank[kSortItems];
 #pragma unroll
@@ -178,7 +191,7 @@ __global__ void __launch_bounds__(kSortThreads, 3) onesweep_kernel(OnesweepParam
   __syncthreads();  // every digit's block-local start is read by other threads below
 
   // decoupled look-back for digit d (digits above the mask are empty everywhere)
-  uint32_t* lb = p.lookback;
+  uint32_t* lb = p.lookback + (size_t)(ticket - tile) * kRadix;  // this segment's chain
   if (tile == 0 || (uint32_t)d > mask) {
     st_relaxed_u32(&lb[(size_t)tile * kRadix + d], kLbPrefix | count);
   } else {
@@ -236,8 +249,8 @@ __global__ void __launch_bounds__(kSortThreads, 3) onesweep_kernel(OnesweepParam
     const uint32_t digit = (k32 >> shift) & mask;
     const uint32_t out = sm.global_base[digit] + (i - sm.block_excl[digit]);
     if (out < n) {  // always true unless a look-back gave up (the status word then says so)
-      p.keys_out[out] = k32;
-      p.vals_out[out] = sm.vals[i];
+      keys_out[out] = k32;
+      vals_out[out] = sm.vals[i];
     }
   }
 }
@@ -248,7 +261,7 @@ __global__ void __launch_bounds__(kSortThreads, 3) onesweep_kernel(OnesweepParam
 // plus a decoupled look-back over the preceding blocks.  Each warp then writes the instances of
 // its 32 Gaussians (one contiguous span) 32 at a time: a 5-step shuffle search finds each
 // instance's Gaussian, so a splat covering hundreds of tiles does not serialise one thread.
-__global__ void __launch_bounds__(kScanBlock) duplicate_kernel(DuplicateParams p) {
+__global__ void __launch_bounds__(kScanBlock) duplicate_kernel(const __grid_constant__ DuplicateParams p) {
   __shared__ uint32_t s_tile;
   __shared__ uint32_t s_warp[kScanBlock / 32];
   __shared__ unsigned long long s_excl;
@@ -260,21 +273,24 @@ __global__ void __launch_bounds__(kScanBlock) duplicate_kernel(DuplicateParams p
   __syncthreads();
   const uint32_t tile = s_tile;
   const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
+  const uint32_t items = (uint32_t)p.P * (uint32_t)p.V;
   const uint32_t i = tile * kScanBlock + threadIdx.x;
-  uint32_t count = 0, g = 0;
-  int rminx = 0, rminy = 0, width = 1;
-  if (i < (uint32_t)p.P) {
+  uint32_t count = 0, g = 0, tile_origin = 0;
+  int pitch = 1, width = 1;
+  if (i < items) {
+    const uint32_t view = (p.V == 1) ? 0u : i / (uint32_t)p.P;  // the order keeps records in their view
     g = p.order[i];
-    const int radius = (g < (uint32_t)p.P) ? p.radii[g] : 0;
+    const int radius = (g - view * (uint32_t)p.P < (uint32_t)p.P) ? p.radii[g] : 0;
     if (radius > 0) {
       const float4 a = p.splat[2 * g];
+      const int gx = p.gx[view];
       int2 rmin, rmax;
-      tile_rect(make_float2(a.x, a.y), radius, p.gx, p.gy, rmin, rmax);
-      rminx = rmin.x;
-      rminy = rmin.y;
+      tile_rect(make_float2(a.x, a.y), radius, gx, p.gy[view], rmin, rmax);
       width = rmax.x - rmin.x;
       count = (uint32_t)width * (uint32_t)(rmax.y - rmin.y);
       if (count == 0) width = 1;
+      pitch = gx;
+      tile_origin = p.tile_base[view] + (uint32_t)rmin.y * (uint32_t)gx + (uint32_t)rmin.x;
     }
   }
   // block inclusive scan of the counts
@@ -344,7 +360,7 @@ __global__ void __launch_bounds__(kScanBlock) duplicate_kernel(DuplicateParams p
   }
   __syncthreads();
   const uint32_t start = (uint32_t)(s_excl + incl_local - count);
-  const uint32_t last_tile = (uint32_t)((p.P + kScanBlock - 1) / kScanBlock) - 1u;
+  const uint32_t last_tile = (items + kScanBlock - 1) / kScanBlock - 1u;
   if (tile == last_tile && threadIdx.x == kScanBlock - 1 && s_excl + block_total != p.hdr->num_rendered64)
     atomicOr(&p.hdr->status, kStatusInconsistent);
 
@@ -361,15 +377,15 @@ __global__ void __launch_bounds__(kScanBlock) duplicate_kernel(DuplicateParams p
       if (s <= o) pos += step;
     }
     const uint32_t o_start = __shfl_sync(kFullMask, start, pos);
-    const int o_rminx = __shfl_sync(kFullMask, rminx, pos);
-    const int o_rminy = __shfl_sync(kFullMask, rminy, pos);
+    const uint32_t o_origin = __shfl_sync(kFullMask, tile_origin, pos);
+    const int o_pitch = __shfl_sync(kFullMask, pitch, pos);
     const int o_width = __shfl_sync(kFullMask, width, pos);
     const uint32_t o_g = __shfl_sync(kFullMask, g, pos);
     if (o < w_end && o < limit) {
       const uint32_t local = o - o_start;
-      const uint32_t ty = (uint32_t)o_rminy + local / (uint32_t)o_width;
-      const uint32_t tx = (uint32_t)o_rminx + local % (uint32_t)o_width;
-      p.tkeys[o] = ty * (uint32_t)p.gx + tx;
+      const uint32_t ry = local / (uint32_t)o_width;
+      const uint32_t rx = local - ry * (uint32_t)o_width;
+      p.tkeys[o] = o_origin + ry * (uint32_t)o_pitch + rx;
       p.tvals[o] = o_g;
     }
   }
@@ -404,19 +420,23 @@ int sm_count() {
 }  // namespace
 
 void launch_histogram(const HistParams& p, int64_t max_items, cudaStream_t s) {
-  const int64_t blocks = std::max<int64_t>(1, std::min<int64_t>((max_items + 255) / 256, sm_count() * 4));
-  histogram_kernel<<<(unsigned)blocks, 256, 0, s>>>(p);
+  const unsigned segs = p.seg_len ? std::max(1u, p.num_segs) : 1u;
+  const int64_t per_seg = p.seg_len ? (int64_t)p.seg_len : max_items;
+  const int64_t blocks = std::max<int64_t>(
+      1, std::min<int64_t>((per_seg + 255) / 256, std::max<int64_t>(1, sm_count() * 4 / segs)));
+  histogram_kernel<<<dim3((unsigned)blocks, segs), 256, 0, s>>>(p);
 }
 
 void launch_onesweep(const OnesweepParams& p, int64_t max_items, cudaStream_t s) {
-  const int64_t blocks = sort_tiles(max_items);
+  const int64_t blocks = p.seg_len ? sort_tiles(p.seg_len) * (int64_t)p.num_segs : sort_tiles(max_items);
   if (blocks <= 0) return;
   onesweep_kernel<<<(unsigned)blocks, kSortThreads, 0, s>>>(p);
 }
 
 void launch_duplicate(const DuplicateParams& p, cudaStream_t s) {
-  if (p.P <= 0) return;
-  duplicate_kernel<<<(p.P + kScanBlock - 1) / kScanBlock, kScanBlock, 0, s>>>(p);
+  const int64_t items = (int64_t)p.P * p.V;
+  if (items <= 0) return;
+  duplicate_kernel<<<(unsigned)((items + kScanBlock - 1) / kScanBlock), kScanBlock, 0, s>>>(p);
 }
 
 void launch_ranges(const RangesParams& p, cudaStream_t s) {

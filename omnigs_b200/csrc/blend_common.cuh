@@ -20,15 +20,43 @@ static_assert(kBlendPx == 1 || kBlendPx == 2 || kBlendPx == 4, "a 16x16 tile spl
 constexpr int kBlendThreads = 256 / kBlendPx;
 constexpr int kBlendWarps = kBlendThreads / 32;
 
+// One 16x16 tile of one view, as a blend block sees it.  The per-pixel pointers are the view's.
+struct TileJob {
+  int tile_x, tile_y;
+  int W, H;
+  uint2 range;              // [begin, end) of the tile's instances in the sorted list
+  const float* bg;          // [3]
+  float* out_color;         // [3,H,W]
+  float* final_T;           // [H*W]
+  uint32_t* n_contrib;      // [H*W]
+  const float* dL_dpix;     // [3,H,W] (backward)
+};
+
+// The sorted instance list and the per-record splat data it points into.
+struct BlendSource {
+  const uint32_t* point_list;  // record index per instance
+  const float4* splat;         // [records][2]
+  const float4* color;         // [records]
+  uint32_t num_records;
+  int64_t capacity;            // instances the list can hold; larger range bounds are rejected
+};
+
+// Tile range read from the ranges table, emptied if inconsistent with the list's capacity.
+__device__ __forceinline__ uint2 checked_range(const uint2* ranges, uint32_t tile, int64_t capacity) {
+  uint2 range = ranges[tile];
+  if (range.y > (uint64_t)capacity || range.x > range.y) range = make_uint2(0, 0);
+  return range;
+}
+
 struct BlendPatch {
   int px, py0;       // this thread's column and first row
   float pxf;         // column as float
   float wcx, wcy;    // centre of the warp's patch
 
-  static __device__ __forceinline__ BlendPatch make() {
+  static __device__ __forceinline__ BlendPatch make(int tile_x, int tile_y) {
     const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
-    const int wx0 = blockIdx.x * 16 + (warp & 1) * 8;
-    const int wy0 = blockIdx.y * 16 + (warp >> 1) * 4 * kBlendPx;
+    const int wx0 = tile_x * 16 + (warp & 1) * 8;
+    const int wy0 = tile_y * 16 + (warp >> 1) * 4 * kBlendPx;
     BlendPatch b;
     b.px = wx0 + (lane & 7);
     b.py0 = wy0 + (lane >> 3);
@@ -66,17 +94,17 @@ __device__ __forceinline__ float splat_power(const float4& a, const float4& b, f
 
 // Stages instances [base, base + cnt) of the tile's list (from the back when reverse: slot t holds
 // position base_hi - 1 - t, with base the exclusive upper end) into shared memory.
-__device__ __forceinline__ void stage_batch(const RenderParams& p, uint32_t range_begin, int base, int cnt,
+__device__ __forceinline__ void stage_batch(const BlendSource& src, uint32_t range_begin, int base, int cnt,
                                             bool reverse, float4* s_a, float4* s_b, float4* s_c,
                                             uint32_t* s_g) {
   for (int t = threadIdx.x; t < cnt; t += kBlendThreads) {
     const uint32_t pos = reverse ? (uint32_t)(base - 1 - t) : (uint32_t)(base + t);
-    const uint32_t g = p.point_list[range_begin + pos];
-    if (g < (uint32_t)p.P) {
+    const uint32_t g = src.point_list[range_begin + pos];
+    if (g < src.num_records) {
       if (s_g) s_g[t] = g;
-      s_a[t] = p.splat[2 * g];
-      s_b[t] = p.splat[2 * g + 1];
-      s_c[t] = p.color[g];
+      s_a[t] = src.splat[2 * g];
+      s_b[t] = src.splat[2 * g + 1];
+      s_c[t] = src.color[g];
     } else {  // unreachable for a consistent instance list; stage a splat that never contributes
       if (s_g) s_g[t] = 0;
       s_a[t] = make_float4(__int_as_float(0x7f800000), 0.f, 0.f, 0.f);
@@ -84,6 +112,31 @@ __device__ __forceinline__ void stage_batch(const RenderParams& p, uint32_t rang
       s_c[t] = make_float4(0.f, 0.f, 0.f, 0.f);
     }
   }
+}
+
+// Block -> (view, tile) of a batched blend launch: blocks run over the views' tiles in the order
+// of tile_base (the host lays the views out heaviest tiles first).
+__device__ __forceinline__ TileJob batch_tile_job(const BatchRenderParams& p, uint32_t block) {
+  int v = p.tile_order[0];
+#pragma unroll 1
+  for (int k = 1; k < p.V; ++k) {
+    const int w = p.tile_order[k];
+    if (p.views[w].tile_base <= block) v = w;
+  }
+  const BatchView& bv = p.views[v];
+  const uint32_t local = block - bv.tile_base;
+  TileJob job;
+  job.tile_y = (int)(local / (uint32_t)bv.gx);
+  job.tile_x = (int)(local - (uint32_t)job.tile_y * (uint32_t)bv.gx);
+  job.W = bv.W;
+  job.H = bv.H;
+  job.range = checked_range(p.ranges, block, p.capacity);
+  job.bg = p.backgrounds + 3 * v;
+  job.out_color = bv.out_color;
+  job.final_T = p.final_T + bv.pixel_base;
+  job.n_contrib = p.n_contrib + bv.pixel_base;
+  job.dL_dpix = bv.dL_dpix;
+  return job;
 }
 
 }  // namespace omnigs

@@ -9,10 +9,10 @@
 #include <vector>
 
 #include "../../include/omnigs_b200.h"
+#include "capi_internal.h"
 #include "kernels.h"
 
 namespace omnigs {
-namespace {
 
 thread_local std::string g_last_error;
 
@@ -30,24 +30,9 @@ int check_launch(const char* what) {
   return OMNIGS_OK;
 }
 
-template <class T>
-T* at(void* base, size_t off) {
-  return reinterpret_cast<T*>(static_cast<unsigned char*>(base) + off);
-}
-template <class T>
-const T* at(const void* base, size_t off) {
-  return reinterpret_cast<const T*>(static_cast<const unsigned char*>(base) + off);
-}
-
-// ---- launch accounting and optional per-stage event timing ----
 std::atomic<uint64_t> g_launches{0};
 std::atomic<bool> g_timing{false};
 std::mutex g_timing_mu;
-struct TimedLaunch {
-  int stage;
-  int kernels;
-  cudaEvent_t start, stop;
-};
 std::vector<TimedLaunch> g_timed;
 std::vector<cudaEvent_t> g_event_pool;
 
@@ -62,26 +47,18 @@ cudaEvent_t take_event() {
   return e;
 }
 
-// Runs `launch` (which enqueues `kernels` kernels on `s`) and accounts for it.
-template <class F>
-void staged(int stage, int kernels, cudaStream_t s, F&& launch) {
-  g_launches.fetch_add((uint64_t)kernels, std::memory_order_relaxed);
-  if (!g_timing.load(std::memory_order_relaxed)) {
-    launch();
-    return;
-  }
-  std::lock_guard<std::mutex> lock(g_timing_mu);
-  TimedLaunch t{stage, kernels, take_event(), take_event()};
-  cudaEventRecord(t.start, s);
-  launch();
-  cudaEventRecord(t.stop, s);
-  g_timed.push_back(t);
+__global__ void begin_render_kernel(GeomHeader* hdr) {
+  atomicAnd(&hdr->status, ~(kStatusCapacity | kStatusInconsistent));
+  const unsigned long long total = hdr->num_rendered64;
+  if (total > (unsigned long long)kMaxInstances) atomicOr(&hdr->status, kStatusOverflow);
+  hdr->num_rendered = (uint32_t)(total > 0xffffffffull ? 0xffffffffull : total);
+  hdr->dup_tile_counter = 0;
+  for (int i = 0; i < kMaxSortPasses; ++i) hdr->sort_tile_counter[i] = 0;
 }
 
-// Buffer (0 or 1) that holds the sorted tile ids / point list after the tile passes.
-int tile_final(int W, int H) { return TileDigits::make(W, H).passes & 1; }
+void launch_begin_render(GeomHeader* hdr, cudaStream_t s) { begin_render_kernel<<<1, 1, 0, s>>>(hdr); }
 
-int validate_common(int P, int D, int M, int W, int H, const float* shs, const float* colors,
+int validate_common(int P, int D, int M, int W, int H, const void* shs, const float* colors,
                     const float* scales, const float* rotations, const float* cov3D,
                     const float* means3D, const float* viewmatrix, const float* campos) {
   if (P < 0) return fail(OMNIGS_ERR_INVALID_ARGUMENT, "P must be >= 0");
@@ -103,6 +80,11 @@ int validate_common(int P, int D, int M, int W, int H, const float* shs, const f
   return OMNIGS_OK;
 }
 
+namespace {
+
+// Buffer (0 or 1) that holds the sorted tile ids / point list after the tile passes.
+int tile_final(int W, int H) { return TileDigits::make(W, H).passes & 1; }
+
 int validate_forward(const OmnigsLonlatForwardArgs* a) {
   if (a == nullptr) return fail(OMNIGS_ERR_INVALID_ARGUMENT, "args is NULL");
   const int rc = validate_common(a->P, a->D, a->M, a->W, a->H, a->shs, a->colors_precomp, a->scales,
@@ -113,15 +95,6 @@ int validate_forward(const OmnigsLonlatForwardArgs* a) {
   if (a->P > 0 && (a->radii == nullptr || a->opacities == nullptr))
     return fail(OMNIGS_ERR_INVALID_ARGUMENT, "radii and opacities are required");
   return OMNIGS_OK;
-}
-
-__global__ void begin_render_kernel(GeomHeader* hdr) {
-  atomicAnd(&hdr->status, ~(kStatusCapacity | kStatusInconsistent));
-  const unsigned long long total = hdr->num_rendered64;
-  if (total > (unsigned long long)kMaxInstances) atomicOr(&hdr->status, kStatusOverflow);
-  hdr->num_rendered = (uint32_t)(total > 0xffffffffull ? 0xffffffffull : total);
-  hdr->dup_tile_counter = 0;
-  for (int i = 0; i < kMaxSortPasses; ++i) hdr->sort_tile_counter[i] = 0;
 }
 
 __global__ void mark_visible_kernel(int P, const float* means3D, const float* vm, int camera_type,
@@ -245,7 +218,7 @@ int omnigs_lonlat_render(const OmnigsLonlatForwardArgs* a, void* geom, size_t ge
   const int64_t depth_tiles = sort_tiles(a->P);
   const int64_t inst_tiles = sort_tiles(BL.capacity);
 
-  staged(OMNIGS_STAGE_OTHER, 1, s, [&] { begin_render_kernel<<<1, 1, 0, s>>>(hdr); });
+  staged(OMNIGS_STAGE_OTHER, 1, s, [&] { launch_begin_render(hdr, s); });
   if (cudaMemsetAsync(at<unsigned char>(geom, GL.dup_scan), 0, GL.zero_end - GL.dup_scan, s) != cudaSuccess ||
       cudaMemsetAsync(hist, 0, sizeof(uint32_t) * kMaxSortPasses * kRadix, s) != cudaSuccess ||
       cudaMemsetAsync(at<uint32_t>(binning, BL.tile_lookback), 0,
@@ -289,8 +262,10 @@ int omnigs_lonlat_render(const OmnigsLonlatForwardArgs* a, void* geom, size_t ge
   uint32_t* tvals[2] = {at<uint32_t>(binning, BL.tvals0), at<uint32_t>(binning, BL.tvals1)};
   DuplicateParams d{};
   d.P = a->P;
-  d.gx = gx;
-  d.gy = gy;
+  d.V = 1;
+  d.gx[0] = gx;
+  d.gy[0] = gy;
+  d.tile_base[0] = 0;
   d.radii = a->radii;
   d.splat = at<float4>(geom, GL.splat);
   d.order = order;

@@ -8,6 +8,9 @@
 
 namespace omnigs {
 
+// Views per batched launch.
+constexpr int kMaxBatchViews = 32;
+
 struct PreprocessParams {
   int P, D, M, W, H, gx, gy;
   const float* means3D;
@@ -30,6 +33,8 @@ struct PreprocessParams {
 };
 
 // Digit histograms of up to kDepthPasses digits of u32 keys.
+// With seg_len > 0 the keys are num_segs independent segments of seg_len items each (the views of
+// a batch) and every segment gets its own histograms, at hist + seg * passes * kRadix.
 struct HistParams {
   const uint32_t* keys;
   uint32_t n_host;             // item count when count_hdr is null
@@ -38,7 +43,9 @@ struct HistParams {
   int passes;
   int shift[kDepthPasses];
   uint32_t mask[kDepthPasses];
-  uint32_t* hist;              // [passes][kRadix], zeroed by the caller
+  uint32_t* hist;              // [segments][passes][kRadix], zeroed by the caller
+  uint32_t seg_len;            // 0: one segment of all items
+  uint32_t num_segs;
 };
 
 // One stable LSD radix pass over (u32 key, u32 value) pairs.
@@ -52,22 +59,31 @@ struct OnesweepParams {
   uint32_t n_host;
   const GeomHeader* count_hdr;
   int64_t capacity;
-  const uint32_t* hist;        // this pass's [kRadix] histogram
+  const uint32_t* hist;        // this pass's [kRadix] histogram (of segment 0)
   uint32_t* lookback;          // [sort tiles][kRadix], zeroed by the caller
   uint32_t* tile_counter;      // zeroed by the caller
   GeomHeader* hdr;             // status bits
+  // Segmented sort (each segment sorted on its own, in place): seg_len items per segment, the
+  // histogram of segment s at hist + s * hist_seg_stride.  seg_len == 0: one segment.
+  uint32_t seg_len;
+  uint32_t num_segs;
+  uint32_t hist_seg_stride;
 };
 
+// duplicateWithKeys over V views (V = 1 for a single view).  Records are view-major (rec = v P + g);
+// instance keys are global tile ids tile_base[v] + ty gx[v] + tx and values record indices.
 struct DuplicateParams {
-  int P, gx, gy;
-  const int* radii;
-  const float4* splat;
-  const uint32_t* order;       // [P] Gaussian indices sorted by (depth bits, index)
+  int P, V;
+  const int* radii;            // [V][P]
+  const float4* splat;         // [V][P][2]
+  const uint32_t* order;       // [V][P] record indices sorted by (view, depth bits, index)
   uint32_t* tkeys;             // [capacity] tile ids
-  uint32_t* tvals;             // [capacity] Gaussian indices
+  uint32_t* tvals;             // [capacity] record indices
   unsigned long long* scan_state;
   int64_t capacity;
   GeomHeader* hdr;
+  int gx[kMaxBatchViews], gy[kMaxBatchViews];
+  uint32_t tile_base[kMaxBatchViews];
 };
 
 struct RangesParams {
@@ -117,6 +133,84 @@ struct PreprocessBackwardParams {
   float* dL_dscales;    // [P,3]
   float* dL_drotations; // [P,4]
 };
+
+// ------------------------------------------------------------------ batched views -------------
+// Many equirect views of one shared Gaussian set.  Per-(view, Gaussian) records are view-major:
+// record index rec = v * P + g.  Global tile ids run over all views: view v owns
+// [tile_base, tile_base + gx * gy); its pixels occupy [pixel_base, pixel_base + W * H) of the
+// per-pixel state arrays.
+struct BatchView {
+  int W, H, gx, gy;
+  uint32_t tile_base;
+  uint32_t pixel_base;
+  float* out_color;             // [3,H,W]
+  const float* dL_dpix;         // [3,H,W] (backward)
+};
+
+struct BatchParams {
+  int P, V, D, M;
+  int sh_bf16;                  // shs holds bf16 instead of fp32 values
+  uint32_t total_tiles;
+  const float* means3D;
+  const float* scales;
+  const float* rotations;
+  const float* opacities;
+  const void* shs;
+  const float* colors_precomp;
+  const float* cov3D_precomp;
+  float scale_modifier;
+  const float* viewmatrices;    // [V][16]
+  const float* campos;          // [V][3]
+  const float* backgrounds;     // [V][3]
+  int* radii;                   // [V][P]
+  float4* splat;                // [V][P][2]
+  float4* color;                // [V][P]
+  float* depth;                 // [V][P]
+  float4* grad_acc;             // [V][P][3]
+  GeomHeader* hdr;
+  unsigned long long* view_rendered;  // [V] instances per view
+  BatchView views[kMaxBatchViews];
+};
+
+// Gradient outputs of the batched backward, summed over the views, plus the densification
+// statistics the trainer accumulates per view (gaussian_mapper.cpp:423-428,
+// gaussian_model.cpp:839-853).  Every non-null output is fully written, except the statistics,
+// which are accumulated into.
+struct BatchGrads {
+  float* dL_dmeans3D;    // [P,3]
+  float* dL_dsh;         // [P,M,3] fp32 (null when there are no SH)
+  float* dL_dopacity;    // [P]
+  float* dL_dscales;     // [P,3]
+  float* dL_drotations;  // [P,4]
+  float* dL_dcolors;     // [P,3] or null (precomputed colours)
+  float* dL_dcov3D;      // [P,6] or null (precomputed covariances)
+  float* grad_accum;     // [P] += |dL/dmean2D.xy| per view where visible, or null
+  float* denom;          // [P] += 1 per view where visible, or null
+  float* max_radii;      // [P] = max(max_radii, radius) over visible views, or null
+};
+
+
+struct BatchRenderParams {
+  int P, V;
+  const uint2* ranges;          // [total tiles]
+  const uint32_t* point_list;   // record indices
+  int64_t capacity;
+  const float4* splat;
+  const float4* color;
+  const float* backgrounds;     // [V][3]
+  float* final_T;               // [total pixels]
+  uint32_t* n_contrib;          // [total pixels]
+  float* grad_acc;              // [V][P][12]
+  uint32_t total_tiles;
+  BatchView views[kMaxBatchViews];
+  uint8_t tile_order[kMaxBatchViews];  // view indices by ascending tile_base
+};
+
+void launch_batch_preprocess(const BatchParams& p, int fp64_poles, cudaStream_t s);
+void launch_batch_render_forward(const BatchRenderParams& p, cudaStream_t s);
+void launch_batch_render_backward(const BatchRenderParams& p, cudaStream_t s);
+void launch_batch_preprocess_backward(const BatchParams& p, const BatchGrads& g, int fp64_poles,
+                                      cudaStream_t s);
 
 void launch_preprocess(const PreprocessParams& p, cudaStream_t s);
 void launch_histogram(const HistParams& p, int64_t max_items, cudaStream_t s);

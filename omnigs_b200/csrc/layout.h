@@ -135,6 +135,45 @@ struct BinningLayout {
   }
 };
 
+// State of a batch of V views over P shared Gaussians (one buffer; the instance lists use a
+// BinningLayout buffer as in the single-view case).  Per-(view, Gaussian) arrays are view-major;
+// per-pixel arrays hold the views' pixels back to back, ranges the views' tiles back to back.
+//
+//   header | instances per view u64[32] | duplicate-scan look-back u64[VP/256] |
+//   depth-sort look-back u32[4][V sort tiles(P)][256] | depth histograms u32[V][4][256] |
+//   radii i32[VP] | splat records float4[2VP] | colour float4[VP] | depth f32[VP] |
+//   depth-sort keys/values u32[4][VP] | gradient accumulators float4[3VP] |
+//   final transmittance f32[pixels] | last contributor u32[pixels] | tile ranges uint2[tiles]
+struct BatchLayout {
+  size_t header, view_rendered, dup_scan, depth_lookback, depth_hist, zero_end, radii, splat, color, depth,
+      dkeys0, dkeys1, dvals0, dvals1, grad_acc, final_T, n_contrib, ranges, total;
+  static BatchLayout make(int64_t P, int V, int64_t pixels, int64_t tiles) {
+    BatchLayout L;
+    const int64_t R = P * V;
+    size_t o = 0;
+    L.header = o; o = align_up(o + sizeof(GeomHeader));
+    L.view_rendered = o; o = align_up(o + sizeof(uint64_t) * 32);
+    L.dup_scan = o; o = align_up(o + sizeof(uint64_t) * ((R + kScanBlock - 1) / kScanBlock));
+    L.depth_lookback = o; o = align_up(o + sizeof(uint32_t) * kDepthPasses * sort_tiles(P) * V * kRadix);
+    L.depth_hist = o; o = align_up(o + sizeof(uint32_t) * V * kDepthPasses * kRadix);
+    L.zero_end = o;  // everything above is cleared before each pass
+    L.radii = o; o = align_up(o + sizeof(int32_t) * R);
+    L.splat = o; o = align_up(o + sizeof(float) * 8 * R);
+    L.color = o; o = align_up(o + sizeof(float) * 4 * R);
+    L.depth = o; o = align_up(o + sizeof(float) * R);
+    L.dkeys0 = o; o = align_up(o + sizeof(uint32_t) * R);
+    L.dkeys1 = o; o = align_up(o + sizeof(uint32_t) * R);
+    L.dvals0 = o; o = align_up(o + sizeof(uint32_t) * R);
+    L.dvals1 = o; o = align_up(o + sizeof(uint32_t) * R);
+    L.grad_acc = o; o = align_up(o + sizeof(float) * 12 * R);
+    L.final_T = o; o = align_up(o + sizeof(float) * pixels);
+    L.n_contrib = o; o = align_up(o + sizeof(uint32_t) * pixels);
+    L.ranges = o; o = align_up(o + sizeof(uint32_t) * 2 * tiles);
+    L.total = o;
+    return L;
+  }
+};
+
 // getHigherMsb (rasterizer_impl.cu:47-62): the reference sorts key bits [0, 32 + bit), i.e. all
 // tile-id bits; the tile passes here cover the same `bit` bits (rasterizer_impl.cu:651-661).
 inline uint32_t higher_msb(uint32_t n);
@@ -145,6 +184,7 @@ struct TileDigits {
   int shift[kTilePasses];
   uint32_t mask[kTilePasses];
   static TileDigits make(int W, int H);
+  static TileDigits from_tiles(uint32_t tiles);
 };
 
 inline uint32_t higher_msb(uint32_t n) {
@@ -162,7 +202,10 @@ inline uint32_t higher_msb(uint32_t n) {
 }
 
 inline TileDigits TileDigits::make(int W, int H) {
-  const uint32_t tiles = (uint32_t)tiles_x(W) * (uint32_t)tiles_y(H);
+  return from_tiles((uint32_t)tiles_x(W) * (uint32_t)tiles_y(H));
+}
+
+inline TileDigits TileDigits::from_tiles(uint32_t tiles) {
   const int bit = (int)higher_msb(tiles);
   TileDigits t{};
   t.passes = (bit + kRadixBits - 1) / kRadixBits;

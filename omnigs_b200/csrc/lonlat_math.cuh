@@ -47,20 +47,27 @@ __device__ __forceinline__ V3 operator*(float s, V3 v) { return V3{s * v.x, s * 
 __device__ __forceinline__ V3 operator/(V3 v, float s) { return V3{v.x / s, v.y / s, v.z / s}; }
 __device__ __forceinline__ float dot3(V3 a, V3 b) { return a.x * b.x + a.y * b.y + a.z * b.z; }
 
-struct Mat3c {
-  float m[3][3];  // m[column][row]
+template <class T>
+struct Mat3 {
+  T m[3][3];  // m[column][row]
 };
-__device__ __forceinline__ Mat3c mat3_cols(float a0, float a1, float a2, float a3, float a4, float a5,
-                                           float a6, float a7, float a8) {
-  Mat3c r;
+using Mat3c = Mat3<float>;
+template <class T>
+__device__ __forceinline__ Mat3<T> mat3_cols_t(T a0, T a1, T a2, T a3, T a4, T a5, T a6, T a7, T a8) {
+  Mat3<T> r;
   r.m[0][0] = a0; r.m[0][1] = a1; r.m[0][2] = a2;
   r.m[1][0] = a3; r.m[1][1] = a4; r.m[1][2] = a5;
   r.m[2][0] = a6; r.m[2][1] = a7; r.m[2][2] = a8;
   return r;
 }
+__device__ __forceinline__ Mat3c mat3_cols(float a0, float a1, float a2, float a3, float a4, float a5,
+                                           float a6, float a7, float a8) {
+  return mat3_cols_t<float>(a0, a1, a2, a3, a4, a5, a6, a7, a8);
+}
 __device__ __forceinline__ Mat3c mat3_identity() { return mat3_cols(1.f, 0.f, 0.f, 0.f, 1.f, 0.f, 0.f, 0.f, 1.f); }
-__device__ __forceinline__ Mat3c mat3_mul(const Mat3c& a, const Mat3c& b) {
-  Mat3c r;
+template <class T>
+__device__ __forceinline__ Mat3<T> mat3_mul(const Mat3<T>& a, const Mat3<T>& b) {
+  Mat3<T> r;
 #pragma unroll
   for (int c = 0; c < 3; ++c)
 #pragma unroll
@@ -68,8 +75,9 @@ __device__ __forceinline__ Mat3c mat3_mul(const Mat3c& a, const Mat3c& b) {
       r.m[c][i] = a.m[0][i] * b.m[c][0] + a.m[1][i] * b.m[c][1] + a.m[2][i] * b.m[c][2];
   return r;
 }
-__device__ __forceinline__ Mat3c mat3_transpose(const Mat3c& a) {
-  Mat3c r;
+template <class T>
+__device__ __forceinline__ Mat3<T> mat3_transpose(const Mat3<T>& a) {
+  Mat3<T> r;
 #pragma unroll
   for (int c = 0; c < 3; ++c)
 #pragma unroll
@@ -162,6 +170,52 @@ __device__ __forceinline__ float3 cov2d_lonlat(const float3& mean, int width, in
   cov.m[0][0] += 0.3f;
   cov.m[1][1] += 0.3f;
   return float3{cov.m[0][0], cov.m[0][1], cov.m[1][1]};
+}
+
+// Gradients of the pixel coordinates with respect to the world-space mean, in FP64: column c of
+// the reference's T = W J (forward.cu:164-176), i.e. g[c][i] = sum_k R^T(i, k) d(p_c)/d(t_k), with
+// the same 1e-7 guards as the FP32 Jacobian.  Used by the precision mode near the poles.
+struct LonlatGradF64 {
+  double gx[3], gy[3];
+};
+__device__ __forceinline__ LonlatGradF64 lonlat_grad_f64(const float3& mean, int width, int height,
+                                                         const float* vm) {
+  const double tx = (double)vm[0] * mean.x + (double)vm[4] * mean.y + (double)vm[8] * mean.z + vm[12];
+  const double ty = (double)vm[1] * mean.x + (double)vm[5] * mean.y + (double)vm[9] * mean.z + vm[13];
+  const double tz = (double)vm[2] * mean.x + (double)vm[6] * mean.y + (double)vm[10] * mean.z + vm[14];
+  const double rxz2 = tx * tx + tz * tz;
+  const double rxz2_inv = 1.0 / (rxz2 + 1e-7);
+  const double rxz = sqrt(rxz2);
+  const double rxz_inv = 1.0 / (rxz + 1e-7);
+  const double rr = rxz2 + ty * ty;
+  const double rr_inv = 1.0 / (rr + 1e-7);
+  const double w2pi = width * 0.5 / 3.14159265358979323846;
+  const double hpi = height / 3.14159265358979323846;
+  const double jx[3] = {w2pi * tz * rxz2_inv, 0.0, -w2pi * tx * rxz2_inv};
+  const double jy[3] = {-hpi * tx * ty * rxz_inv * rr_inv, hpi * rxz * rr_inv, -hpi * tz * ty * rxz_inv * rr_inv};
+  LonlatGradF64 g;
+#pragma unroll
+  for (int i = 0; i < 3; ++i) {
+    g.gx[i] = (double)vm[4 * i] * jx[0] + (double)vm[4 * i + 1] * jx[1] + (double)vm[4 * i + 2] * jx[2];
+    g.gy[i] = (double)vm[4 * i] * jy[0] + (double)vm[4 * i + 1] * jy[1] + (double)vm[4 * i + 2] * jy[2];
+  }
+  return g;
+}
+
+// u^T Sigma v for the symmetric 3D covariance stored as (xx, xy, xz, yy, yz, zz).
+__device__ __forceinline__ double sym_form_f64(const float* s, const double* u, const double* v) {
+  const double su0 = s[0] * u[0] + s[1] * u[1] + s[2] * u[2];
+  const double su1 = s[1] * u[0] + s[3] * u[1] + s[4] * u[2];
+  const double su2 = s[2] * u[0] + s[4] * u[1] + s[5] * u[2];
+  return su0 * v[0] + su1 * v[1] + su2 * v[2];
+}
+
+// cov2d_lonlat in FP64: (a, b, c) of the screen-space covariance including the 0.3 low-pass.
+__device__ __forceinline__ double3 cov2d_lonlat_f64(const float3& mean, int width, int height,
+                                                    const float* cov3D, const float* viewmatrix) {
+  const LonlatGradF64 g = lonlat_grad_f64(mean, width, height, viewmatrix);
+  return make_double3(sym_form_f64(cov3D, g.gx, g.gx) + 0.3, sym_form_f64(cov3D, g.gx, g.gy),
+                      sym_form_f64(cov3D, g.gy, g.gy) + 0.3);
 }
 
 // View-dependent colour from degree-<=3 SH (forward.cu:30-83).  `sh` points at this Gaussian's

@@ -59,44 +59,42 @@ struct PixelState {
   float last_alpha;
 };
 
-__global__ void __launch_bounds__(kBlendThreads) render_backward_kernel(RenderParams p) {
+__device__ __forceinline__ void blend_backward_tile(const TileJob& job, const BlendSource& src, float* grad_acc) {
   __shared__ float4 s_a[kBatch];
   __shared__ float4 s_b[kBatch];
   __shared__ float4 s_c[kBatch];
   __shared__ uint32_t s_g[kBatch];
   __shared__ uint32_t s_warp_last[kBlendWarps];
-  const BlendPatch patch = BlendPatch::make();
+  const BlendPatch patch = BlendPatch::make(job.tile_x, job.tile_y);
   const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
-
-  uint2 range = p.ranges[blockIdx.y * p.gx + blockIdx.x];
-  if (range.y > (uint64_t)p.capacity || range.x > range.y) range = make_uint2(0, 0);
+  const uint2 range = job.range;
   const uint32_t n = range.y - range.x;
 
-  const int64_t HW = (int64_t)p.H * p.W;
+  const int64_t HW = (int64_t)job.H * job.W;
   PixelState ps[kBlendPx];
   uint32_t thread_last = 0;
 #pragma unroll
   for (int i = 0; i < kBlendPx; ++i) {
     PixelState& s = ps[i];
-    const bool in = patch.inside(i, p.W, p.H);
-    const int64_t pix = in ? patch.pixel(i, p.W) : 0;
-    s.T_final = in ? p.final_T[pix] : 0.f;
+    const bool in = patch.inside(i, job.W, job.H);
+    const int64_t pix = in ? patch.pixel(i, job.W) : 0;
+    s.T_final = in ? job.final_T[pix] : 0.f;
     s.T = s.T_final;
-    s.last_contributor = in ? p.n_contrib[pix] : 0u;
+    s.last_contributor = in ? job.n_contrib[pix] : 0u;
     if (s.last_contributor > n) s.last_contributor = n;
     thread_last = max(thread_last, s.last_contributor);
-    s.dpix[0] = in ? p.dL_dpix[pix] : 0.f;
-    s.dpix[1] = in ? p.dL_dpix[HW + pix] : 0.f;
-    s.dpix[2] = in ? p.dL_dpix[2 * HW + pix] : 0.f;
+    s.dpix[0] = in ? job.dL_dpix[pix] : 0.f;
+    s.dpix[1] = in ? job.dL_dpix[HW + pix] : 0.f;
+    s.dpix[2] = in ? job.dL_dpix[2 * HW + pix] : 0.f;
     s.bg_dot_dpixel = 0.f;
 #pragma unroll
-    for (int ch = 0; ch < 3; ch++) s.bg_dot_dpixel += p.bg[ch] * s.dpix[ch];
+    for (int ch = 0; ch < 3; ch++) s.bg_dot_dpixel += job.bg[ch] * s.dpix[ch];
     s.accum_rec[0] = s.accum_rec[1] = s.accum_rec[2] = 0.f;
     s.last_color[0] = s.last_color[1] = s.last_color[2] = 0.f;
     s.last_alpha = 0.f;
   }
-  const float ddelx_dx = 0.5 * p.W;
-  const float ddely_dy = 0.5 * p.H;
+  const float ddelx_dx = 0.5 * job.W;
+  const float ddely_dy = 0.5 * job.H;
 
   const uint32_t warp_last = __reduce_max_sync(kFullMask, thread_last);
   if (lane == 0) s_warp_last[warp] = warp_last;
@@ -108,7 +106,7 @@ __global__ void __launch_bounds__(kBlendThreads) render_backward_kernel(RenderPa
   for (int hi = (int)block_last; hi > 0; hi -= kBatch) {
     const int cnt = min(kBatch, hi);
     __syncthreads();
-    stage_batch(p, range.x, hi, cnt, /*reverse=*/true, s_a, s_b, s_c, s_g);
+    stage_batch(src, range.x, hi, cnt, /*reverse=*/true, s_a, s_b, s_c, s_g);
     __syncthreads();
     for (int k = 0; k * 32 < cnt; ++k) {
       const int j = k * 32 + lane;
@@ -166,7 +164,7 @@ __global__ void __launch_bounds__(kBlendThreads) render_backward_kernel(RenderPa
         }
         const unsigned cm = __ballot_sync(kFullMask, contrib);
         if (cm == 0) continue;
-        float* acc = p.grad_acc + 12 * (size_t)s_g[jj];
+        float* acc = grad_acc + 12 * (size_t)s_g[jj];
         if ((cm & (cm - 1)) == 0) {  // one contributing lane: add its values directly
           if (contrib) {
 #pragma unroll
@@ -180,11 +178,39 @@ __global__ void __launch_bounds__(kBlendThreads) render_backward_kernel(RenderPa
   }
 }
 
+// One view: block (x, y) back-propagates tile (x, y).
+__global__ void __launch_bounds__(kBlendThreads) render_backward_kernel(RenderParams p) {
+  TileJob job;
+  job.tile_x = blockIdx.x;
+  job.tile_y = blockIdx.y;
+  job.W = p.W;
+  job.H = p.H;
+  job.range = checked_range(p.ranges, blockIdx.y * p.gx + blockIdx.x, p.capacity);
+  job.bg = p.bg;
+  job.out_color = nullptr;
+  job.final_T = p.final_T;
+  job.n_contrib = p.n_contrib;
+  job.dL_dpix = p.dL_dpix;
+  blend_backward_tile(job, BlendSource{p.point_list, p.splat, p.color, (uint32_t)p.P, p.capacity}, p.grad_acc);
+}
+
+// All views of a batch in one launch: block b back-propagates global tile b.
+__global__ void __launch_bounds__(kBlendThreads) batch_render_backward_kernel(const __grid_constant__ BatchRenderParams p) {
+  const TileJob job = batch_tile_job(p, blockIdx.x);
+  blend_backward_tile(job, BlendSource{p.point_list, p.splat, p.color, (uint32_t)p.P * (uint32_t)p.V, p.capacity},
+                      p.grad_acc);
+}
+
 }  // namespace
 
 void launch_render_backward(const RenderParams& p, cudaStream_t s) {
   if (p.gx <= 0 || p.gy <= 0) return;
   render_backward_kernel<<<dim3(p.gx, p.gy), kBlendThreads, 0, s>>>(p);
+}
+
+void launch_batch_render_backward(const BatchRenderParams& p, cudaStream_t s) {
+  if (p.total_tiles == 0) return;
+  batch_render_backward_kernel<<<p.total_tiles, kBlendThreads, 0, s>>>(p);
 }
 
 }  // namespace omnigs

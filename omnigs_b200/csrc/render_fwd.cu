@@ -19,15 +19,13 @@
 namespace omnigs {
 namespace {
 
-__global__ void __launch_bounds__(kBlendThreads) render_forward_kernel(RenderParams p) {
+__device__ __forceinline__ void blend_forward_tile(const TileJob& job, const BlendSource& src) {
   __shared__ float4 s_a[kBatch];  // x, y, conic a, conic b
   __shared__ float4 s_b[kBatch];  // conic c, opacity, cull half-width, cull half-height
   __shared__ float4 s_c[kBatch];  // r, g, b, clamp bits
-  const BlendPatch patch = BlendPatch::make();
+  const BlendPatch patch = BlendPatch::make(job.tile_x, job.tile_y);
   const int lane = threadIdx.x & 31;
-
-  uint2 range = p.ranges[blockIdx.y * p.gx + blockIdx.x];
-  if (range.y > (uint64_t)p.capacity || range.x > range.y) range = make_uint2(0, 0);
+  const uint2 range = job.range;
   const int n = (int)(range.y - range.x);
 
   bool done[kBlendPx];
@@ -35,7 +33,7 @@ __global__ void __launch_bounds__(kBlendThreads) render_forward_kernel(RenderPar
   uint32_t last_contributor[kBlendPx];
 #pragma unroll
   for (int i = 0; i < kBlendPx; ++i) {
-    done[i] = !patch.inside(i, p.W, p.H);
+    done[i] = !patch.inside(i, job.W, job.H);
     T[i] = 1.0f;
     C0[i] = C1[i] = C2[i] = 0.f;
     last_contributor[i] = 0;
@@ -49,7 +47,7 @@ __global__ void __launch_bounds__(kBlendThreads) render_forward_kernel(RenderPar
 
   for (int base = 0; base < n; base += kBatch) {
     if (__syncthreads_and(all_done())) break;
-    stage_batch(p, range.x, base, min(kBatch, n - base), /*reverse=*/false, s_a, s_b, s_c, nullptr);
+    stage_batch(src, range.x, base, min(kBatch, n - base), /*reverse=*/false, s_a, s_b, s_c, nullptr);
     __syncthreads();
     const int cnt = min(kBatch, n - base);
     bool warp_done = __all_sync(kFullMask, all_done());
@@ -92,17 +90,39 @@ __global__ void __launch_bounds__(kBlendThreads) render_forward_kernel(RenderPar
     }
   }
 
-  const int64_t HW = (int64_t)p.H * p.W;
+  const int64_t HW = (int64_t)job.H * job.W;
 #pragma unroll
   for (int i = 0; i < kBlendPx; ++i) {
-    if (!patch.inside(i, p.W, p.H)) continue;
-    const int64_t pix = patch.pixel(i, p.W);
-    p.final_T[pix] = T[i];
-    p.n_contrib[pix] = last_contributor[i];
-    p.out_color[pix] = __fmaf_rn(T[i], p.bg[0], C0[i]);
-    p.out_color[HW + pix] = __fmaf_rn(T[i], p.bg[1], C1[i]);
-    p.out_color[2 * HW + pix] = __fmaf_rn(T[i], p.bg[2], C2[i]);
+    if (!patch.inside(i, job.W, job.H)) continue;
+    const int64_t pix = patch.pixel(i, job.W);
+    job.final_T[pix] = T[i];
+    job.n_contrib[pix] = last_contributor[i];
+    job.out_color[pix] = __fmaf_rn(T[i], job.bg[0], C0[i]);
+    job.out_color[HW + pix] = __fmaf_rn(T[i], job.bg[1], C1[i]);
+    job.out_color[2 * HW + pix] = __fmaf_rn(T[i], job.bg[2], C2[i]);
   }
+}
+
+// One view: block (x, y) blends tile (x, y).
+__global__ void __launch_bounds__(kBlendThreads) render_forward_kernel(RenderParams p) {
+  TileJob job;
+  job.tile_x = blockIdx.x;
+  job.tile_y = blockIdx.y;
+  job.W = p.W;
+  job.H = p.H;
+  job.range = checked_range(p.ranges, blockIdx.y * p.gx + blockIdx.x, p.capacity);
+  job.bg = p.bg;
+  job.out_color = p.out_color;
+  job.final_T = p.final_T;
+  job.n_contrib = p.n_contrib;
+  job.dL_dpix = nullptr;
+  blend_forward_tile(job, BlendSource{p.point_list, p.splat, p.color, (uint32_t)p.P, p.capacity});
+}
+
+// All views of a batch in one launch: block b blends global tile b.
+__global__ void __launch_bounds__(kBlendThreads) batch_render_forward_kernel(const __grid_constant__ BatchRenderParams p) {
+  const TileJob job = batch_tile_job(p, blockIdx.x);
+  blend_forward_tile(job, BlendSource{p.point_list, p.splat, p.color, (uint32_t)p.P * (uint32_t)p.V, p.capacity});
 }
 
 }  // namespace
@@ -110,6 +130,11 @@ __global__ void __launch_bounds__(kBlendThreads) render_forward_kernel(RenderPar
 void launch_render_forward(const RenderParams& p, cudaStream_t s) {
   if (p.gx <= 0 || p.gy <= 0) return;
   render_forward_kernel<<<dim3(p.gx, p.gy), kBlendThreads, 0, s>>>(p);
+}
+
+void launch_batch_render_forward(const BatchRenderParams& p, cudaStream_t s) {
+  if (p.total_tiles == 0) return;
+  batch_render_forward_kernel<<<p.total_tiles, kBlendThreads, 0, s>>>(p);
 }
 
 }  // namespace omnigs

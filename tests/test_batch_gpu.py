@@ -1,0 +1,165 @@
+"""GPU parity of the batched multi-view path (omnigs_batch_* through the C ABI).
+
+The single-view path is pinned bit for bit to the reference rasterizer (test_reference_gpu.py), so
+the batch is checked against it: every view's instance count, last contributors, transmittance and
+image are identical to a single-view forward of that view; the parameter gradients equal the sum
+of the single-view backwards (1e-5 normwise relative: the sum runs in a different order); the
+densification statistics equal the trainer's per-view accumulation.  BF16 SH storage is checked
+against the FP32 path fed with the same bf16-rounded coefficients (images bit-identical), and the
+FP64 pole mode against the FP64 oracle.
+"""
+import numpy as np
+import pytest
+import torch
+
+import helpers
+import oracle
+from omnigs_b200 import batch, capi, lonlat, scenes
+
+pytestmark = pytest.mark.gpu
+
+GRAD_RTOL = 1e-5
+
+
+def _rel(a, b):
+    a, b = helpers.to_np(a).astype(np.float64), helpers.to_np(b).astype(np.float64)
+    return np.abs(a - b).max() / max(np.abs(b).max(), 1e-30)
+
+
+def _views(sizes, seed):
+    """Identity pose for the first view, then positions within a 2 m cube and random yaw/pitch."""
+    rng = np.random.Generator(np.random.PCG64(seed + 10))
+    views = [scenes.identity_view(*sizes[0])]
+    for w, h in sizes[1:]:
+        R = scenes.rotation_yaw_pitch(rng.uniform(-np.pi, np.pi), np.radians(rng.uniform(-30, 30)))
+        views.append(scenes.make_view(w, h, rng.uniform(-1.0, 1.0, 3), R))
+    return views
+
+
+def _plain(gt, view, dpix, bg):
+    cam = lonlat.Camera.from_view(view, background=bg)
+    return helpers.run_cuda(gt, cam, torch.from_numpy(dpix).cuda())
+
+
+def _batch(gt, views, dpix_list, bg, fp64_poles=False, capacity=None):
+    cams = batch.BatchCameras.from_views(views, background=bg)
+    images, per_view, state = batch.render_batch(gt, cams, fp64_poles=fp64_poles, capacity=capacity)
+    grads = batch.BatchGradients.empty(gt.P, gt.M, gt.means3D.device, stats=True)
+    dl = [torch.from_numpy(d).cuda() for d in dpix_list]
+    state.backward(gt, cams, dl, grads, fp64_poles=fp64_poles)
+    torch.cuda.synchronize()
+    return images, per_view, state, grads
+
+
+@pytest.mark.parametrize("sizes,P,seed", [
+    ([(512, 256)], 10_000, 0),
+    ([(512, 256), (1024, 512), (96, 48), (500, 250)], 20_000, 1),
+    ([(2048, 1024), (512, 256), (3072, 1536)], 60_000, 2),
+])
+def test_batch_matches_single_views(cuda, sizes, P, seed):
+    g = scenes.make_gaussians(P, seed=seed)
+    gt = lonlat.GaussianTensors.from_numpy(g)
+    views = _views(sizes, seed)
+    bg = (0.1, 0.2, 0.3)
+    dpix = [scenes.upstream_grad(w, h, seed=seed + 20 + i) for i, (w, h) in enumerate(sizes)]
+    images, per_view, state, grads = _batch(gt, views, dpix, bg)
+    sv = state.state_view()
+    sums = {k: 0.0 for k in ("dL_dmeans3D", "dL_dsh", "dL_dopacity", "dL_dscales", "dL_drotations")}
+    stat_norm = torch.zeros(P, device=cuda, dtype=torch.float64)
+    stat_cnt = torch.zeros(P, device=cuda, dtype=torch.float64)
+    max_r = torch.zeros(P, device=cuda, dtype=torch.int32)
+    for v, view in enumerate(views):
+        cu = _plain(gt, view, dpix[v], bg)
+        assert per_view[v] == cu["num_rendered"]
+        torch.testing.assert_close(sv["radii"][v], cu["radii"], rtol=0, atol=0)
+        torch.testing.assert_close(sv["n_contrib"][v], cu["n_contrib"], rtol=0, atol=0)
+        torch.testing.assert_close(sv["final_T"][v], cu["final_T"], rtol=0, atol=0)
+        torch.testing.assert_close(images[v], cu["image"], rtol=0, atol=0)
+        for k in sums:
+            sums[k] = sums[k] + getattr(cu["grads"], k).double()
+        vis = cu["radii"] > 0
+        m2 = cu["grads"].dL_dmeans2D.double()
+        stat_norm += torch.where(vis, torch.linalg.norm(m2[:, :2], dim=1), 0.0)
+        stat_cnt += vis.double()
+        max_r = torch.maximum(max_r, torch.where(vis, cu["radii"], 0))
+    for k, ref in sums.items():
+        assert _rel(getattr(grads, k), ref) < GRAD_RTOL, k
+    assert _rel(grads.grad_accum[:, 0], stat_norm) < 1e-5
+    torch.testing.assert_close(grads.denom[:, 0].double(), stat_cnt, rtol=0, atol=0)
+    torch.testing.assert_close(grads.max_radii, max_r.float(), rtol=0, atol=0)
+
+
+def test_bf16_sh_equals_fp32_path_on_rounded_coefficients(cuda):
+    g = scenes.make_gaussians(20_000, seed=3)
+    gt = lonlat.GaussianTensors.from_numpy(g)
+    sh16 = gt.shs.to(torch.bfloat16)
+    g16 = lonlat.GaussianTensors(means3D=gt.means3D, opacities=gt.opacities, shs=sh16,
+                                 scales=gt.scales, rotations=gt.rotations)
+    grounded = lonlat.GaussianTensors(means3D=gt.means3D, opacities=gt.opacities, shs=sh16.float(),
+                                      scales=gt.scales, rotations=gt.rotations)
+    views = [scenes.identity_view(512, 256), scenes.make_view(1024, 512, (0.3, -0.2, 0.5))]
+    dpix = [scenes.upstream_grad(w.width, w.height, seed=5 + i) for i, w in enumerate(views)]
+    cams = batch.BatchCameras.from_views(views)
+    out = {}
+    for name, gg in (("bf16", g16), ("fp32", grounded)):
+        images, per_view, state = batch.render_batch(gg, cams)
+        grads = batch.BatchGradients.empty(gg.P, gg.M, cuda)
+        state.backward(gg, cams, [torch.from_numpy(d).cuda() for d in dpix], grads)
+        torch.cuda.synchronize()
+        out[name] = (images, per_view, grads)
+    assert out["bf16"][1] == out["fp32"][1]
+    for a, b in zip(out["bf16"][0], out["fp32"][0]):
+        torch.testing.assert_close(a, b, rtol=0, atol=0)
+    # same coefficients, same formulas: the two kernel instantiations may fuse a few products
+    # differently, so gradients agree to FP32 rounding rather than bit for bit
+    for k in ("dL_dmeans3D", "dL_dsh", "dL_dopacity", "dL_dscales", "dL_drotations"):
+        assert _rel(getattr(out["bf16"][2], k), getattr(out["fp32"][2], k)) < GRAD_RTOL, k
+
+
+def test_capacity_overflow_resumes(cuda):
+    g = scenes.make_gaussians(10_000, seed=4)
+    gt = lonlat.GaussianTensors.from_numpy(g)
+    views = [scenes.identity_view(512, 256), scenes.make_view(256, 128, (0.5, 0.0, 0.0))]
+    cams = batch.BatchCameras.from_views(views)
+    ref_images, ref_per, _ = batch.render_batch(gt, cams)
+    small = batch.BatchState(gt.P, cams.sizes, capacity=1000)
+    images = [torch.empty(3, h, w, device=cuda) for w, h in cams.sizes]
+    small.forward(gt, cams, images)
+    n, per, st = small.status()
+    assert st & capi.STATUS_CAPACITY and n == sum(ref_per) and per == ref_per
+    small.resize_capacity(n)
+    small.render(gt, cams, images)
+    n2, per2, st2 = small.status()
+    assert st2 == 0 and per2 == ref_per
+    for a, b in zip(images, ref_images):
+        torch.testing.assert_close(a, b, rtol=0, atol=0)
+
+
+def test_fp64_poles_tracks_the_fp64_oracle_closer(cuda):
+    """Pole-heavy scene: the conics of Gaussians beyond 85 degrees from the FP64 pole mode are
+    closer to the FP64 oracle's than the FP32 path's; elsewhere both are identical."""
+    P, W, H = 20_000, 1024, 512
+    g = scenes.make_gaussians(P, seed=6, pole_fraction=0.3, pole_min_lat_deg=84.0)
+    gt = lonlat.GaussianTensors.from_numpy(g)
+    view = scenes.identity_view(W, H)
+    cams = batch.BatchCameras.from_views([view])
+    _, _, s32 = batch.render_batch(gt, cams, fp64_poles=False)
+    _, _, s64 = batch.render_batch(gt, cams, fp64_poles=True)
+    pre = oracle.preprocess(g.means3D, g.scales, g.rotations, g.opacities, g.shs, view.viewmatrix,
+                            view.campos, W, H)
+    lat = np.degrees(np.arcsin(np.abs(g.means3D[:, 1]) / np.linalg.norm(g.means3D, axis=1)))
+    c32 = helpers.to_np(s32.state_view()["splat"][0])[:, 2:5].astype(np.float64)
+    c64 = helpers.to_np(s64.state_view()["splat"][0])[:, [2, 3, 4]].astype(np.float64)
+    r32 = helpers.to_np(s32.state_view()["radii"][0])
+    r64 = helpers.to_np(s64.state_view()["radii"][0])
+    ref = pre["conic_opacity"][:, :3]
+    vis = (r32 > 0) & (r64 > 0) & (pre["radii"] > 0)
+    pole, rest = vis & (lat > 85.5), vis & (lat < 84.5)
+    assert pole.sum() > 100
+    np.testing.assert_array_equal(c32[rest], c64[rest])
+    scale = np.abs(ref).max(1)
+    e32 = (np.abs(c32 - ref).max(1) / scale)[pole]
+    e64 = (np.abs(c64 - ref).max(1) / scale)[pole]
+    msg = f"FP32 max {e32.max():.3g} mean {e32.mean():.3g}; FP64 poles max {e64.max():.3g} mean {e64.mean():.3g}"
+    assert e64.mean() <= e32.mean(), msg
+    assert e64.max() <= max(e32.max(), 1e-6), msg

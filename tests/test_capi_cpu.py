@@ -160,3 +160,57 @@ def test_views_follow_reference_conventions():
     # the camera centre maps to the camera-space origin; campos is that centre
     np.testing.assert_allclose((Tcw @ np.array([1.0, 2.0, 3.0, 1.0]))[:3], 0.0, atol=1e-5)
     np.testing.assert_allclose(v.campos, [1.0, 2.0, 3.0], atol=1e-5)
+
+
+def test_batch_state_bytes_validates_the_views():
+    one = capi.batch_state_bytes(1000, [(512, 256)])
+    two = capi.batch_state_bytes(1000, [(512, 256), (1024, 512)])
+    assert 0 < one < two
+    assert capi.batch_state_bytes(2000, [(512, 256)]) > one
+    assert capi.batch_state_bytes(1000, []) == 0
+    assert capi.batch_state_bytes(1000, [(64, 32)] * (capi.MAX_BATCH_VIEWS + 1)) == 0
+    assert capi.batch_state_bytes(1000, [(64, 32)] * capi.MAX_BATCH_VIEWS) > 0
+    assert capi.batch_state_bytes(1000, [(0, 256)]) == 0
+    assert capi.batch_state_bytes(-1, [(512, 256)]) == 0
+
+
+def _fake_batch(V=2, **over):
+    fake = 0x10000
+    views = (capi.BatchView * max(V, 1))()
+    for v in range(V):
+        views[v].W, views[v].H = 64 * (v + 1), 32 * (v + 1)
+        views[v].out_color = fake
+        views[v].dL_dout_color = fake
+    a = capi.BatchArgs()
+    a.P, a.D, a.M, a.V = 10, 3, 16, V
+    for f in ("means3D", "shs", "opacities", "scales", "rotations", "viewmatrices", "campos", "backgrounds"):
+        setattr(a, f, fake)
+    a.scale_modifier = 1.0
+    a.views = views
+    for k, v in over.items():
+        setattr(a, k, v)
+    return a, views
+
+
+@pytest.mark.parametrize("over,code", [
+    (dict(V=0), 1), (dict(V=capi.MAX_BATCH_VIEWS + 1), 1), (dict(sh_dtype=2), 1), (dict(fp64_poles=3), 1),
+    (dict(M=17), 1), (dict(D=4), 1), (dict(backgrounds=None), 1), (dict(opacities=None), 1),
+    (dict(colors_precomp=0x10000), 1), (dict(cov3D_precomp=0x10000), 1),
+])
+def test_batch_entry_points_reject_bad_arguments_before_device_work(over, code):
+    a, keep = _fake_batch(**over)
+    L = capi.lib()
+    assert L.omnigs_batch_forward(ctypes.byref(a), 0x10000, 1 << 40, 0x10000, 1 << 40, None) == code
+    assert L.omnigs_last_error()
+    g = capi.BatchGrads()
+    for f, _ in capi.BatchGrads._fields_:
+        setattr(g, f, 0x10000)
+    assert L.omnigs_batch_backward(ctypes.byref(a), ctypes.byref(g), 0x10000, 1 << 40, 0x10000, 1 << 40,
+                                   None) == code
+
+
+def test_batch_state_too_small_is_rejected():
+    a, keep = _fake_batch()
+    L = capi.lib()
+    need = capi.batch_state_bytes(10, [(64, 32), (128, 64)])
+    assert L.omnigs_batch_forward(ctypes.byref(a), 0x10000, need - 1, 0x10000, 1 << 40, None) == 2
