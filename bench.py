@@ -53,6 +53,7 @@ def parse():
     ap.add_argument("--impl", default="omnigs", choices=["omnigs", "reference"])
     ap.add_argument("--no-cpu-baseline", action="store_true")
     ap.add_argument("--no-e2e", action="store_true")
+    ap.add_argument("--no-batch", action="store_true", help="skip the batched multi-view leg")
     # smaller cases for profiling captures only; bench lines use the defaults
     ap.add_argument("--gaussians", type=int, default=P_GAUSS)
     ap.add_argument("--width", type=int, default=WIDTH)
@@ -208,6 +209,85 @@ def run_reference(args, rank, world):
                                        "path, so this is the FP64 oracle restating its algorithm"},
             "e2e": {"value": value, "unit": UNIT, "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0}}
     print(json.dumps(line), flush=True)
+
+
+# ---------------------------------------------------------------- batched views ----------------
+BATCH_VIEWS = 16
+
+
+def run_batched(args, gt, dev, plain_views_per_s):
+    """Batched fwd+bwd of 16 uneven equirect views over the shared 1M-Gaussian set, one launch per
+    stage for the whole batch, the step captured in a CUDA graph and replayed (poses and upstream
+    gradients live at fixed device addresses; instance counts stay on the device).  Timed with SH
+    stored as BF16 (the precision mode's storage) and, for comparison, as FP32."""
+    import torch
+
+    from omnigs_b200 import batch, capi, lonlat, scenes
+
+    views = scenes.random_views(BATCH_VIEWS, scenes.BATCH_RESOLUTIONS, seed=1, cube=2.0, pitch_deg=30.0)
+    cams = batch.BatchCameras.from_views(views, dev)
+    dl = [torch.from_numpy(scenes.upstream_grad(v.width, v.height, seed=100 + i)).to(dev)
+          for i, v in enumerate(views)]
+    images = [torch.empty(3, v.height, v.width, device=dev) for v in views]
+    pixels = sum(v.width * v.height for v in views)
+    results = {}
+    stream = torch.cuda.Stream(dev)
+    for name, shs in (("bf16", gt.shs.to(torch.bfloat16)), ("fp32", gt.shs)):
+        gg = lonlat.GaussianTensors(means3D=gt.means3D, opacities=gt.opacities, shs=shs,
+                                    scales=gt.scales, rotations=gt.rotations)
+        _, per_view, sizing = batch.render_batch(gg, cams)
+        total = sum(per_view)
+        del sizing
+        state = batch.BatchState(gg.P, cams.sizes, total + total // 8 + 4096, dev)
+        grads = batch.BatchGradients.empty(gg.P, gg.M, dev, stats=True)
+
+        def step():
+            state.forward(gg, cams, images)
+            state.backward(gg, cams, dl, grads)
+
+        with torch.cuda.stream(stream):
+            for _ in range(2):
+                step()
+        torch.cuda.synchronize()
+        graph = torch.cuda.CUDAGraph()
+        with torch.cuda.graph(graph, stream=stream):
+            step()
+        for _ in range(args.warmup):
+            graph.replay()
+        torch.cuda.synchronize()
+        n, per2, st = state.status()
+        assert st == 0 and per2 == per_view, (st, per2, per_view)
+        cur = torch.cuda.current_stream(dev)
+        ev0, ev1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+        ev0.record(cur)
+        for _ in range(args.steps):
+            graph.replay()
+        ev1.record(cur)
+        torch.cuda.synchronize()
+        ms = ev0.elapsed_time(ev1) / args.steps
+        del graph
+        # per-stage device times from eager (uncaptured) steps with the library's event timing
+        k = max(1, args.steps // 4)
+        capi.timing_enable(True)
+        for _ in range(k):
+            step()
+        torch.cuda.synchronize()
+        stages = capi.timing_read()
+        capi.timing_enable(False)
+        results[name] = {
+            "views_per_s": round(BATCH_VIEWS / (ms / 1000.0), 3), "ms_per_view": round(ms / BATCH_VIEWS, 4),
+            "ms_per_step": round(ms, 4),
+            "speedup_vs_plain_fp32": round(BATCH_VIEWS / (ms / 1000.0) / plain_views_per_s, 3),
+            "num_rendered": int(n), "gpu_launches_per_step": sum(v[1] for v in stages.values()) // k,
+            "stages_ms_per_step": {s: round(v[0] / k, 4) for s, v in stages.items() if v[1]},
+        }
+        del state, grads
+        torch.cuda.empty_cache()
+    return {"workload": f"{BATCH_VIEWS} equirect views, resolutions drawn from {scenes.BATCH_RESOLUTIONS}, "
+                        "positions uniform in a 2 m cube, random yaw, pitch +-30 deg, 1M shared Gaussians, "
+                        "fwd+bwd of the whole batch per step, CUDA graph replay",
+            "views": BATCH_VIEWS, "pixels_per_step": pixels, "sizes": [list(s) for s in cams.sizes],
+            "sh_bf16": results["bf16"], "sh_fp32": results["fp32"]}
 
 
 # ---------------------------------------------------------------- omnigs arm --------------------
@@ -371,6 +451,10 @@ def run_omnigs(args, rank, world, local_rank):
                "d2h_bytes_per_step": int(h_img.numel() * 4 + 4),
                "api": "RasterizeGaussiansCUDA + RasterizeGaussiansBackwardCUDA (LibTorch layer)"}
 
+    batched = None
+    if world == 1 and not args.no_batch and (P, W, H) == (P_GAUSS, WIDTH, HEIGHT):
+        batched = run_batched(args, gt, dev, value)
+
     cpu = None
     if rank == 0 and world == 1 and not args.no_cpu_baseline:
         cpu = cpu_baseline(g, view, dpix_np)
@@ -386,7 +470,8 @@ def run_omnigs(args, rank, world, local_rank):
                            "num_rendered": n0, "visible": V, "parallelism": f"dp{world} (views)",
                            "l2": "inputs larger than L2 (SH alone 192 MB > 126 MB), no flush"},
                 "gpu_launches": int(launches), "clocks": clocks.summary(), "roofline": roofline,
-                "roofline_fp32": roofline_fp32, "kernels": kernels, "e2e": e2e, "cpu_baseline": cpu}
+                "roofline_fp32": roofline_fp32, "kernels": kernels, "e2e": e2e, "batched": batched,
+                "cpu_baseline": cpu}
         print(json.dumps(line), flush=True)
 
 
