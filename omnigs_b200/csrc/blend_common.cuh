@@ -92,6 +92,22 @@ __device__ __forceinline__ float splat_power(const float4& a, const float4& b, f
   return __fsub_rn(__fmul_rn(-0.5f, quad), __fmul_rn(cb_dx, d.y));
 }
 
+// Packed f32x2 arithmetic (one instruction for both lanes, each rounded as its scalar form).
+__device__ __forceinline__ float2 f2(float a) { return make_float2(a, a); }
+__device__ __forceinline__ float2 add2(float2 a, float2 b) { return __fadd2_rn(a, b); }
+__device__ __forceinline__ float2 sub2(float2 a, float2 b) { return __fadd2_rn(a, make_float2(-b.x, -b.y)); }
+__device__ __forceinline__ float2 mul2(float2 a, float2 b) { return __fmul2_rn(a, b); }
+__device__ __forceinline__ float2 fma2(float2 a, float2 b, float2 c) { return __ffma2_rn(a, b, c); }
+
+// splat_power for two pixels of one column (offsets (dx, dy.x) and (dx, dy.y)), lane by lane
+// bit-identical to splat_power.
+__device__ __forceinline__ float2 splat_power2(const float4& a, const float4& b, float dx, float2 dy) {
+  const float ca_dx = __fmul_rn(a.z, dx), cb_dx = __fmul_rn(a.w, dx);
+  const float2 cc_dy = mul2(f2(b.x), dy);
+  const float2 quad = fma2(f2(ca_dx), f2(dx), mul2(cc_dy, dy));
+  return sub2(mul2(f2(-0.5f), quad), mul2(f2(cb_dx), dy));
+}
+
 // Stages instances [base, base + cnt) of the tile's list (from the back when reverse: slot t holds
 // position base_hi - 1 - t, with base the exclusive upper end) into shared memory.
 __device__ __forceinline__ void stage_batch(const BlendSource& src, uint32_t range_begin, int base, int cnt,
