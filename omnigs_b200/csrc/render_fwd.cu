@@ -4,9 +4,10 @@
 // alpha = min(0.99, o exp(power)), the 1/255 skip, the T < 1e-4 stop), so the image, final
 // transmittance and last-contributor index are identical for the same sorted instance list.
 // What changes is the work around it:
-//  * a thread owns kBlendPx pixels of one column (rows 4 apart), a warp an 8 x (4 kBlendPx) patch;
-//    the per-splat shared-memory reads, loop control and votes are paid once per thread, not
-//    once per pixel, and the thread's pixels give the scheduler independent work;
+//  * a thread owns two pixels of one column (rows 4 apart), a warp an 8 x 8 patch; the per-splat
+//    shared-memory reads, loop control and votes are paid once per thread, not once per pixel,
+//    and the two pixels' arithmetic runs in packed f32x2 instructions (each lane rounded exactly
+//    as the scalar operation, so results are unchanged);
 //  * for each staged batch a warp ballots which splats' alpha-support boxes (computed in the
 //    preprocess) touch its patch and iterates only over those, so pairs that the reference rejects
 //    pixel by pixel are skipped a warp at a time;
@@ -20,6 +21,7 @@ namespace omnigs {
 namespace {
 
 __device__ __forceinline__ void blend_forward_tile(const TileJob& job, const BlendSource& src) {
+  static_assert(kBlendPx == 2, "the forward blend packs a thread's two pixels into f32x2 lanes");
   __shared__ float4 s_a[kBatch];  // x, y, conic a, conic b
   __shared__ float4 s_b[kBatch];  // conic c, opacity, cull half-width, cull half-height
   __shared__ float4 s_c[kBatch];  // r, g, b, clamp bits
@@ -28,29 +30,18 @@ __device__ __forceinline__ void blend_forward_tile(const TileJob& job, const Ble
   const uint2 range = job.range;
   const int n = (int)(range.y - range.x);
 
-  bool done[kBlendPx];
-  float T[kBlendPx], C0[kBlendPx], C1[kBlendPx], C2[kBlendPx];
-  uint32_t last_contributor[kBlendPx];
-#pragma unroll
-  for (int i = 0; i < kBlendPx; ++i) {
-    done[i] = !patch.inside(i, job.W, job.H);
-    T[i] = 1.0f;
-    C0[i] = C1[i] = C2[i] = 0.f;
-    last_contributor[i] = 0;
-  }
-  auto all_done = [&] {
-    bool d = true;
-#pragma unroll
-    for (int i = 0; i < kBlendPx; ++i) d = d && done[i];
-    return d;
-  };
+  // lane x: row py0, lane y: row py0 + 4
+  bool done0 = !patch.inside(0, job.W, job.H), done1 = !patch.inside(1, job.W, job.H);
+  float2 T = f2(1.0f), C0 = f2(0.f), C1 = f2(0.f), C2 = f2(0.f);
+  uint32_t lc0 = 0, lc1 = 0;
+  const float2 pyf = make_float2(patch.pyf(0), patch.pyf(1));
 
   for (int base = 0; base < n; base += kBatch) {
-    if (__syncthreads_and(all_done())) break;
+    if (__syncthreads_and(done0 && done1)) break;
     stage_batch(src, range.x, base, min(kBatch, n - base), /*reverse=*/false, s_a, s_b, s_c, nullptr);
     __syncthreads();
     const int cnt = min(kBatch, n - base);
-    bool warp_done = __all_sync(kFullMask, all_done());
+    bool warp_done = __all_sync(kFullMask, done0 && done1);
     for (int k = 0; k * 32 < cnt && !warp_done; ++k) {
       const int j = k * 32 + lane;
       bool hit = false;
@@ -59,30 +50,40 @@ __device__ __forceinline__ void blend_forward_tile(const TileJob& job, const Ble
       while (m) {
         const int jj = k * 32 + __ffs(m) - 1;
         m &= m - 1;
-        const float4 a = s_a[jj];
-        const float4 b = s_b[jj];
-#pragma unroll
-        for (int i = 0; i < kBlendPx; ++i) {
-          if (done[i]) continue;
-          const float2 d = {a.x - patch.pxf, a.y - patch.pyf(i)};
-          const float power = splat_power(a, b, d);
-          if (power > 0.0f) continue;
-          const float alpha = fminf(0.99f, b.y * expf(power));
-          if (alpha < 1.0f / 255.0f) continue;
-          const float test_T = T[i] * (1 - alpha);
-          if (test_T < 0.0001f) {
-            done[i] = true;
-            continue;
+        if (!(done0 && done1)) {
+          const float4 a = s_a[jj];
+          const float4 b = s_b[jj];
+          const float dx = a.x - patch.pxf;
+          const float2 dy = sub2(f2(a.y), pyf);
+          const float2 power = splat_power2(a, b, dx, dy);
+          const float2 alpha = make_float2(fminf(0.99f, b.y * expf(power.x)), fminf(0.99f, b.y * expf(power.y)));
+          bool act0 = !done0 && !(power.x > 0.0f) && !(alpha.x < 1.0f / 255.0f);
+          bool act1 = !done1 && !(power.y > 0.0f) && !(alpha.y < 1.0f / 255.0f);
+          if (act0 || act1) {
+            const float2 test_T = mul2(T, sub2(f2(1.0f), alpha));
+            // a pixel whose transmittance would fall below 1e-4 stops without this splat
+            if (act0 && test_T.x < 0.0001f) {
+              done0 = true;
+              act0 = false;
+            }
+            if (act1 && test_T.y < 0.0001f) {
+              done1 = true;
+              act1 = false;
+            }
+            const float2 ae = make_float2(act0 ? alpha.x : 0.f, act1 ? alpha.y : 0.f);
+            const float4 c = s_c[jj];
+            // C += colour * alpha * T, rounded as the reference's compiled blend (fused add);
+            // a pixel without this splat adds exactly 0
+            C0 = fma2(mul2(f2(c.x), ae), T, C0);
+            C1 = fma2(mul2(f2(c.y), ae), T, C1);
+            C2 = fma2(mul2(f2(c.z), ae), T, C2);
+            T = make_float2(act0 ? test_T.x : T.x, act1 ? test_T.y : T.y);
+            const uint32_t idx = (uint32_t)(base + jj + 1);
+            lc0 = act0 ? idx : lc0;
+            lc1 = act1 ? idx : lc1;
           }
-          const float4 c = s_c[jj];
-          // C += colour * alpha * T, rounded as the reference's compiled blend (fused add)
-          C0[i] = __fmaf_rn(__fmul_rn(c.x, alpha), T[i], C0[i]);
-          C1[i] = __fmaf_rn(__fmul_rn(c.y, alpha), T[i], C1[i]);
-          C2[i] = __fmaf_rn(__fmul_rn(c.z, alpha), T[i], C2[i]);
-          T[i] = test_T;
-          last_contributor[i] = (uint32_t)(base + jj + 1);
         }
-        if (__all_sync(kFullMask, all_done())) {
+        if (__all_sync(kFullMask, done0 && done1)) {
           warp_done = true;
           break;
         }
@@ -91,15 +92,16 @@ __device__ __forceinline__ void blend_forward_tile(const TileJob& job, const Ble
   }
 
   const int64_t HW = (int64_t)job.H * job.W;
+  const float Ts[2] = {T.x, T.y}, Cs[3][2] = {{C0.x, C0.y}, {C1.x, C1.y}, {C2.x, C2.y}};
+  const uint32_t lcs[2] = {lc0, lc1};
 #pragma unroll
-  for (int i = 0; i < kBlendPx; ++i) {
+  for (int i = 0; i < 2; ++i) {
     if (!patch.inside(i, job.W, job.H)) continue;
     const int64_t pix = patch.pixel(i, job.W);
-    job.final_T[pix] = T[i];
-    job.n_contrib[pix] = last_contributor[i];
-    job.out_color[pix] = __fmaf_rn(T[i], job.bg[0], C0[i]);
-    job.out_color[HW + pix] = __fmaf_rn(T[i], job.bg[1], C1[i]);
-    job.out_color[2 * HW + pix] = __fmaf_rn(T[i], job.bg[2], C2[i]);
+    job.final_T[pix] = Ts[i];
+    job.n_contrib[pix] = lcs[i];
+#pragma unroll
+    for (int ch = 0; ch < 3; ++ch) job.out_color[ch * HW + pix] = __fmaf_rn(Ts[i], job.bg[ch], Cs[ch][i]);
   }
 }
 

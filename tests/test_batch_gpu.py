@@ -3,7 +3,8 @@
 The single-view path is pinned bit for bit to the reference rasterizer (test_reference_gpu.py), so
 the batch is checked against it: every view's instance count, last contributors, transmittance and
 image are identical to a single-view forward of that view; the parameter gradients equal the sum
-of the single-view backwards (1e-5 normwise relative: the sum runs in a different order); the
+of the single-view backwards within 1e-4 normwise relative (the per-splat accumulators are summed
+with float atomics in run-dependent order, and the batch sums the views in another order); the
 densification statistics equal the trainer's per-view accumulation.  BF16 SH storage is checked
 against the FP32 path fed with the same bf16-rounded coefficients (images bit-identical), and the
 FP64 pole mode against the FP64 oracle.
@@ -18,7 +19,7 @@ from omnigs_b200 import batch, capi, lonlat, scenes
 
 pytestmark = pytest.mark.gpu
 
-GRAD_RTOL = 1e-5
+GRAD_RTOL = 1e-4
 
 
 def _rel(a, b):
