@@ -45,7 +45,9 @@ __device__ __forceinline__ uint32_t item_count(const GeomHeader* count_hdr, uint
 }
 
 // ---------------------------------------------------------------- digit histograms ------------
-__global__ void __launch_bounds__(256) histogram_kernel(HistParams p) {
+constexpr int kHistUnroll = 4;  // keys per thread loaded before any of them is counted
+
+__global__ void __launch_bounds__(256) histogram_kernel(const __grid_constant__ HistParams p) {
   __shared__ uint32_t s_hist[kDepthPasses][kRadix];
   for (int i = threadIdx.x; i < kDepthPasses * kRadix; i += blockDim.x) (&s_hist[0][0])[i] = 0;
   __syncthreads();
@@ -53,15 +55,26 @@ __global__ void __launch_bounds__(256) histogram_kernel(HistParams p) {
   const size_t seg_base = (size_t)blockIdx.y * n;  // gridDim.y segments
   const int lane = threadIdx.x & 31;
   const uint32_t stride = gridDim.x * blockDim.x;
-  // whole warps iterate together so that match.any sees all 32 lanes
-  for (uint32_t base = blockIdx.x * blockDim.x + (threadIdx.x & ~31u); base < n; base += stride) {
-    const uint32_t i = base + lane;
-    const bool valid = i < n;
-    const uint32_t key = valid ? p.keys[seg_base + i] : 0u;
-    for (int q = 0; q < p.passes; ++q) {
-      const uint32_t digit = (key >> p.shift[q]) & p.mask[q];
-      const unsigned peers = __match_any_sync(kFullMask, valid ? digit : (0x10000u | lane));
-      if (valid && lane == __ffs(peers) - 1) atomicAdd(&s_hist[q][digit], (uint32_t)__popc(peers));
+  // Whole warps iterate together so that match.any sees all 32 lanes; each thread first loads
+  // kHistUnroll keys (independent loads in flight), then counts them.
+  for (uint32_t base = blockIdx.x * blockDim.x + (threadIdx.x & ~31u); base < n; base += stride * kHistUnroll) {
+    uint32_t key[kHistUnroll];
+    bool valid[kHistUnroll];
+#pragma unroll
+    for (int u = 0; u < kHistUnroll; ++u) {
+      const uint32_t i = base + u * stride + lane;
+      valid[u] = i < n;
+      key[u] = valid[u] ? p.keys[seg_base + i] : 0u;
+    }
+#pragma unroll
+    for (int q = 0; q < kDepthPasses; ++q) {
+      if (q >= p.passes) break;
+#pragma unroll
+      for (int u = 0; u < kHistUnroll; ++u) {
+        const uint32_t digit = (key[u] >> p.shift[q]) & p.mask[q];
+        const unsigned peers = __match_any_sync(kFullMask, valid[u] ? digit : (0x10000u | lane));
+        if (valid[u] && lane == __ffs(peers) - 1) atomicAdd(&s_hist[q][digit], (uint32_t)__popc(peers));
+      }
     }
   }
   __syncthreads();
@@ -423,7 +436,8 @@ void launch_histogram(const HistParams& p, int64_t max_items, cudaStream_t s) {
   const unsigned segs = p.seg_len ? std::max(1u, p.num_segs) : 1u;
   const int64_t per_seg = p.seg_len ? (int64_t)p.seg_len : max_items;
   const int64_t blocks = std::max<int64_t>(
-      1, std::min<int64_t>((per_seg + 255) / 256, std::max<int64_t>(1, sm_count() * 4 / segs)));
+      1, std::min<int64_t>((per_seg + 256 * kHistUnroll - 1) / (256 * kHistUnroll),
+                           std::max<int64_t>(1, sm_count() * 4 / segs)));
   histogram_kernel<<<dim3((unsigned)blocks, segs), 256, 0, s>>>(p);
 }
 
