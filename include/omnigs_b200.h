@@ -270,6 +270,73 @@ typedef struct OmnigsBatchStateView {
 int omnigs_batch_state_view(const void* state, int P, int V, const int* W, const int* H,
                             OmnigsBatchStateView* out);
 
+/* ---------------------------------------------------------------- training step --------------
+ * The kernels around the rasterizer in the reference's training iteration
+ * (GaussianMapper::trainForOneIteration, src/gaussian_mapper.cpp:384-432).
+ *
+ * L1 + D-SSIM loss with its image gradient (include/loss_utils.h:30-131): for images [C,H,W],
+ * using rows [0, rows) (the reference's skip-bottom slice, gaussian_mapper.cpp:389-398; rows = H
+ * for the whole image), writes loss[0] = (1 - lambda) L1 + lambda (1 - SSIM), loss[1] = L1,
+ * loss[2] = SSIM (device floats) and dL_dimage (zero in rows >= `rows`).  SSIM uses the
+ * reference's 11x11 Gaussian window (sigma 1.5), zero padding and C1 = 0.01^2, C2 = 0.03^2.  The
+ * workspace is caller-owned device memory of omnigs_l1_dssim_workspace_bytes(C, H, W). */
+size_t omnigs_l1_dssim_workspace_bytes(int C, int H, int W);
+int omnigs_l1_dssim(const float* image, const float* gt, int C, int H, int W, int rows, float lambda_dssim,
+                    float* dL_dimage, float* loss, void* workspace, size_t workspace_bytes,
+                    omnigs_stream_t stream);
+
+/* Raw (optimised) Gaussian parameters (GaussianModel, src/gaussian_model.cpp:54-77). */
+typedef struct OmnigsGaussianParams {
+  int P, M;              /* Gaussians; SH coefficients per Gaussian (1 DC + M - 1 rest), M <= 16 */
+  float* xyz;            /* [P,3] */
+  float* features_dc;    /* [P,1,3] */
+  float* features_rest;  /* [P,M-1,3] */
+  float* opacity;        /* [P,1], before the sigmoid */
+  float* scaling;        /* [P,3], log of the scales */
+  float* rotation;       /* [P,4], quaternion (r, x, y, z) before normalisation */
+} OmnigsGaussianParams;
+
+/* Adam first and second moments, one pair per parameter array (same shapes). */
+typedef struct OmnigsAdamState {
+  float *m_xyz, *v_xyz, *m_dc, *v_dc, *m_rest, *v_rest, *m_opacity, *v_opacity;
+  float *m_scaling, *v_scaling, *m_rotation, *v_rotation;
+} OmnigsAdamState;
+
+/* Activated values the rasterizer reads: means3D (may alias xyz), SH [P,M,3] as fp32 or bf16
+ * (shs_bf16 = 1), sigmoid(opacity), exp(scaling), normalize(rotation). */
+typedef struct OmnigsActivated {
+  float* means3D;
+  void* shs;
+  int shs_bf16;
+  float* opacities;
+  float* scales;
+  float* rotations;
+} OmnigsActivated;
+
+/* Adam hyper-parameters in DEVICE memory, read when the kernel runs (so a captured graph replays
+ * with the caller's updated step and learning rates).  lr[] per parameter group in the
+ * reference's order (gaussian_model.cpp:534-541): xyz, f_dc, f_rest, opacity, scaling, rotation.
+ * The values are doubles, as torch's AdamOptions holds them: the kernel forms the float
+ * coefficients beta, 1 - beta, lr / (1 - beta1^step) and sqrt(1 - beta2^step) in double and rounds
+ * them once, as torch does.  step is the 1-based step count of the bias corrections. */
+typedef struct OmnigsAdamHyper {
+  double lr[6];
+  double beta1, beta2, eps;
+  int64_t step;
+} OmnigsAdamHyper;
+
+/* Writes the activated values of `params` (the first forward of a run). */
+int omnigs_activate(const OmnigsGaussianParams* params, const OmnigsActivated* act, omnigs_stream_t stream);
+
+/* One Adam step of every parameter group (torch::optim::Adam as set up at
+ * gaussian_model.cpp:485-518, no weight decay) from the rasterizer's gradients with respect to
+ * the activated values, with the activation backward fused in; then refreshes `act`.  `act` must
+ * hold the activation of the current parameters (omnigs_activate or the previous step). */
+int omnigs_adam_step(const OmnigsGaussianParams* params, const OmnigsAdamState* state, const OmnigsActivated* act,
+                     const float* dL_dmeans3D, const float* dL_dsh, const float* dL_dopacity,
+                     const float* dL_dscales, const float* dL_drotations, const OmnigsAdamHyper* hyper,
+                     omnigs_stream_t stream);
+
 /* Visibility marks.  camera_type 3: every Gaussian (markAllVisible, rasterizer_impl.cu:82-90);
  * camera_type 1: the pinhole near test p_view.z > 0.2 (checkFrustum, rasterizer_impl.cu:66-78,
  * auxiliary.h:166-196).  present is a [P] byte array. */

@@ -33,7 +33,7 @@ NVCC_FLAGS = ["-O3", "-std=c++17", "-lineinfo", "-Xcompiler", "-fPIC", "--expt-r
               "-Xptxas", "-warn-spills"]
 
 CU_SOURCES = ["preprocess.cu", "binning.cu", "render_fwd.cu", "render_bwd.cu",
-              "preprocess_bwd.cu", "batch.cu", "capi.cu", "batch_capi.cu", "noalloc.cu"]
+              "preprocess_bwd.cu", "batch.cu", "train.cu", "capi.cu", "batch_capi.cu", "noalloc.cu"]
 HEADERS = glob.glob(os.path.join(CSRC, "*.h")) + glob.glob(os.path.join(CSRC, "*.cuh")) + \
     [os.path.join(ROOT, "include", "omnigs_b200.h")]
 TORCH_SOURCES = ["torch/rasterize_points.cpp", "torch/gaussian_rasterizer.cpp", "torch/bindings.cpp"]

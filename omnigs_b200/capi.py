@@ -97,6 +97,26 @@ class BatchStateView(ctypes.Structure):
                 ("tile_base", ctypes.c_int64 * MAX_BATCH_VIEWS), ("tile_passes", _i)]
 
 
+class GaussianParams(ctypes.Structure):
+    _fields_ = [("P", _i), ("M", _i), ("xyz", _vp), ("features_dc", _vp), ("features_rest", _vp),
+                ("opacity", _vp), ("scaling", _vp), ("rotation", _vp)]
+
+
+class AdamState(ctypes.Structure):
+    _fields_ = [(n, _vp) for n in ("m_xyz", "v_xyz", "m_dc", "v_dc", "m_rest", "v_rest", "m_opacity",
+                                   "v_opacity", "m_scaling", "v_scaling", "m_rotation", "v_rotation")]
+
+
+class Activated(ctypes.Structure):
+    _fields_ = [("means3D", _vp), ("shs", _vp), ("shs_bf16", _i), ("opacities", _vp), ("scales", _vp),
+                ("rotations", _vp)]
+
+
+class AdamHyper(ctypes.Structure):
+    _fields_ = [("lr", ctypes.c_double * 6), ("beta1", ctypes.c_double), ("beta2", ctypes.c_double),
+                ("eps", ctypes.c_double), ("step", ctypes.c_int64)]
+
+
 # every symbol include/omnigs_b200.h declares
 EXPORTED = ["omnigs_version", "omnigs_last_error", "omnigs_lonlat_geom_bytes",
             "omnigs_lonlat_image_bytes", "omnigs_lonlat_binning_bytes",
@@ -107,7 +127,8 @@ EXPORTED = ["omnigs_version", "omnigs_last_error", "omnigs_lonlat_geom_bytes",
             "omnigs_kernel_launches", "omnigs_lonlat_geom_view", "omnigs_lonlat_binning_view",
             "omnigs_lonlat_image_view", "omnigs_batch_state_bytes", "omnigs_batch_forward",
             "omnigs_batch_render", "omnigs_batch_backward", "omnigs_batch_read_status",
-            "omnigs_batch_state_view"]
+            "omnigs_batch_state_view", "omnigs_l1_dssim_workspace_bytes", "omnigs_l1_dssim",
+            "omnigs_activate", "omnigs_adam_step"]
 
 _lib = None
 
@@ -158,6 +179,12 @@ def lib() -> ctypes.CDLL:
                                                ctypes.POINTER(ctypes.c_int64),
                                                ctypes.POINTER(ctypes.c_uint32), _vp]
         L.omnigs_batch_state_view.argtypes = [_vp, _i, _i, ip, ip, ctypes.POINTER(BatchStateView)]
+        L.omnigs_l1_dssim_workspace_bytes.restype = ctypes.c_size_t
+        L.omnigs_l1_dssim_workspace_bytes.argtypes = [_i, _i, _i]
+        L.omnigs_l1_dssim.argtypes = [_vp, _vp, _i, _i, _i, _i, _f, _vp, _vp, _vp, ctypes.c_size_t, _vp]
+        L.omnigs_activate.argtypes = [ctypes.POINTER(GaussianParams), ctypes.POINTER(Activated), _vp]
+        L.omnigs_adam_step.argtypes = [ctypes.POINTER(GaussianParams), ctypes.POINTER(AdamState),
+                                       ctypes.POINTER(Activated), _vp, _vp, _vp, _vp, _vp, _vp, _vp]
         _lib = L
     return _lib
 

@@ -214,3 +214,27 @@ def test_batch_state_too_small_is_rejected():
     L = capi.lib()
     need = capi.batch_state_bytes(10, [(64, 32), (128, 64)])
     assert L.omnigs_batch_forward(ctypes.byref(a), 0x10000, need - 1, 0x10000, 1 << 40, None) == 2
+
+
+def test_loss_workspace_and_validation():
+    L = capi.lib()
+    assert L.omnigs_l1_dssim_workspace_bytes(3, 1024, 2048) >= 3 * 3 * 1024 * 2048 * 4
+    assert L.omnigs_l1_dssim_workspace_bytes(0, 10, 10) == 0
+    f = 0x10000
+    big = 1 << 40
+    assert L.omnigs_l1_dssim(f, f, 3, 64, 32, 65, 0.2, f, f, f, big, None) == 1   # rows > H
+    assert L.omnigs_l1_dssim(f, f, 3, 64, 32, 64, 1.5, f, f, f, big, None) == 1   # lambda outside [0, 1]
+    assert L.omnigs_l1_dssim(None, f, 3, 64, 32, 64, 0.2, f, f, f, big, None) == 1
+    assert L.omnigs_l1_dssim(f, f, 3, 64, 32, 64, 0.2, f, f, f, 16, None) == 2    # workspace too small
+
+
+def test_adam_validation():
+    L = capi.lib()
+    prm, st, act = capi.GaussianParams(), capi.AdamState(), capi.Activated()
+    prm.P, prm.M = 10, 17
+    assert L.omnigs_adam_step(ctypes.byref(prm), ctypes.byref(st), ctypes.byref(act), *([0x10000] * 6),
+                              None) == 1
+    prm.M = 16  # pointers still NULL
+    assert L.omnigs_adam_step(ctypes.byref(prm), ctypes.byref(st), ctypes.byref(act), *([0x10000] * 6),
+                              None) == 1
+    assert L.omnigs_activate(ctypes.byref(prm), ctypes.byref(act), None) == 1
