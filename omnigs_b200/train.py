@@ -3,9 +3,10 @@
 ``GaussianModelState`` holds the reference model's raw parameters (xyz, f_dc, f_rest, opacity
 before the sigmoid, log scaling, unnormalised rotation; src/gaussian_model.cpp:54-77), their Adam
 moments, the activated values the rasterizer reads, and the device-resident Adam hyper-parameters.
-``BatchTrainStep`` is one data-parallel-free training iteration over a batch of views: batched
-forward, per-view loss and image gradient, batched backward, Adam step -- all asynchronous, so the
-whole step can be captured once in a CUDA graph and replayed (``capture``).
+``BatchTrainStep`` is one training iteration over a batch of views: batched forward, per-view loss
+and image gradient, batched backward, (across ranks: one gradient all-reduce,
+``sharding.GradientReducer``), Adam step -- all asynchronous, so the whole step can be captured
+once in a CUDA graph and replayed (``capture``).
 """
 from __future__ import annotations
 
@@ -15,7 +16,7 @@ import math
 import numpy as np
 import torch
 
-from . import batch, capi
+from . import batch, capi, sharding
 from .lonlat import GaussianTensors
 
 # learning rates of the reference's lonlat configurations (cfg/lonlat/*.yaml: Optimization.*),
@@ -138,7 +139,8 @@ class BatchTrainStep:
     Adam.  ``losses`` [V,3] holds each view's (loss, l1, ssim) on the device after a step."""
 
     def __init__(self, model: GaussianModelState, cams: batch.BatchCameras, targets, capacity: int,
-                 lambda_dssim: float = 0.2, D: int = 3, fp64_poles: bool = False):
+                 lambda_dssim: float = 0.2, D: int = 3, fp64_poles: bool = False, process_group=None,
+                 data_parallel: bool = False):
         dev = model.xyz.device
         self.model, self.cams, self.targets = model, cams, targets
         self.lambda_dssim, self.D, self.fp64_poles = lambda_dssim, D, fp64_poles
@@ -149,7 +151,12 @@ class BatchTrainStep:
         W = max(w for w, _ in cams.sizes)
         H = max(h for _, h in cams.sizes)
         self.workspace = l1_dssim_workspace(3, H, W, dev)
-        self.grads = batch.BatchGradients.empty(model.P, model.M, dev, stats=True)
+        # data parallel (one process per GPU, views sharded with sharding.assign_views): the step's
+        # gradients and densification statistics are combined across ranks before Adam
+        self.reducer = sharding.GradientReducer(model.P, model.M, dev, stats=True, group=process_group) \
+            if data_parallel else None
+        self.grads = self.reducer.grads if self.reducer else batch.BatchGradients.empty(model.P, model.M, dev,
+                                                                                        stats=True)
         self.graph = None
 
     def run(self, stream=None):
@@ -161,6 +168,8 @@ class BatchTrainStep:
                      loss=self.losses[v], workspace=self.workspace, stream=stream)
         self.state.backward(g, self.cams, self.dimages, self.grads, D=self.D, fp64_poles=self.fp64_poles,
                             stream=stream)
+        if self.reducer is not None:
+            self.reducer.reduce()
         gr = self.grads
         self.model.adam_step(gr.dL_dmeans3D, gr.dL_dsh, gr.dL_dopacity, gr.dL_dscales, gr.dL_drotations,
                              stream=stream)
