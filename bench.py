@@ -54,6 +54,7 @@ def parse():
     ap.add_argument("--no-cpu-baseline", action="store_true")
     ap.add_argument("--no-e2e", action="store_true")
     ap.add_argument("--no-batch", action="store_true", help="skip the batched multi-view leg")
+    ap.add_argument("--no-extra", action="store_true", help="skip the precision and peak-memory legs")
     # smaller cases for profiling captures only; bench lines use the defaults
     ap.add_argument("--gaussians", type=int, default=P_GAUSS)
     ap.add_argument("--width", type=int, default=WIDTH)
@@ -215,7 +216,7 @@ def run_reference(args, rank, world):
 BATCH_VIEWS = 16
 
 
-def run_batched(args, gt, dev, plain_views_per_s):
+def run_batched(args, g, gt, dev, plain_views_per_s):
     """Batched fwd+bwd of 16 uneven equirect views over the shared 1M-Gaussian set, one launch per
     stage for the whole batch, the step captured in a CUDA graph and replayed (poses and upstream
     gradients live at fixed device addresses; instance counts stay on the device).  Timed with SH
@@ -283,11 +284,148 @@ def run_batched(args, gt, dev, plain_views_per_s):
         }
         del state, grads
         torch.cuda.empty_cache()
+    results["train_step"] = run_train_step(args, g, gt, cams, dev)
     return {"workload": f"{BATCH_VIEWS} equirect views, resolutions drawn from {scenes.BATCH_RESOLUTIONS}, "
                         "positions uniform in a 2 m cube, random yaw, pitch +-30 deg, 1M shared Gaussians, "
                         "fwd+bwd of the whole batch per step, CUDA graph replay",
             "views": BATCH_VIEWS, "pixels_per_step": pixels, "sizes": [list(s) for s in cams.sizes],
-            "sh_bf16": results["bf16"], "sh_fp32": results["fp32"]}
+            "sh_bf16": results["bf16"], "sh_fp32": results["fp32"], "train_step": results["train_step"]}
+
+
+def run_train_step(args, g, gt, cams, dev):
+    """The whole training iteration over the 16-view batch (forward, L1 + 0.2 D-SSIM per view,
+    backward with densification statistics, fused Adam; SH in BF16), captured in one CUDA graph."""
+    import torch
+
+    from omnigs_b200 import batch, capi, train
+
+    targets, per_view, _ = batch.render_batch(gt, cams)
+    total = sum(per_view)
+    model = train.GaussianModelState.from_activated(g, device=dev, sh_bf16=True)
+    stepper = train.BatchTrainStep(model, cams, targets, capacity=total + total // 4 + 4096)
+    stepper.run()
+    torch.cuda.synchronize()
+    stepper.capture()
+    for _ in range(args.warmup):
+        stepper.replay()
+    torch.cuda.synchronize()
+    cur = torch.cuda.current_stream(dev)
+    ev0, ev1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+    ev0.record(cur)
+    for _ in range(args.steps):
+        stepper.replay()
+    ev1.record(cur)
+    torch.cuda.synchronize()
+    ms = ev0.elapsed_time(ev1) / args.steps
+    n, _, st = stepper.status()
+    assert st == 0, st
+    # eager step with stage timing: loss and Adam run under the "other" stage
+    capi.timing_enable(True)
+    stepper.run()
+    torch.cuda.synchronize()
+    stages = capi.timing_read()
+    capi.timing_enable(False)
+    del stepper
+    return {"ms_per_step": round(ms, 4), "views_per_s": round(BATCH_VIEWS / (ms / 1000.0), 3),
+            "sh": "bf16", "graph": True,
+            "stages_ms_one_step": {k: round(v[0], 4) for k, v in stages.items() if v[1]},
+            "note": "loss + Adam appear under 'other'"}
+
+
+def run_precision(args, dev):
+    """Precision configuration: 6M Gaussians, 30 % beyond 80 deg latitude, one 4096x2048 view;
+    fwd+bwd ms/view of the plain FP32 path vs the precision mode (BF16 SH + FP64 poles)."""
+    import torch
+
+    from omnigs_b200 import batch, lonlat, scenes
+
+    P, W, H = 6_000_000, 4096, 2048
+    g = scenes.make_gaussians(P, seed=4, pole_fraction=0.3)
+    gt = lonlat.GaussianTensors.from_numpy(g, dev)
+    view = scenes.identity_view(W, H)
+    dpix = torch.from_numpy(scenes.upstream_grad(W, H, seed=4)).to(dev)
+    out = {}
+    # plain FP32 single-view path
+    cam = lonlat.Camera.from_view(view, dev)
+    _, radii0, n0, _ = lonlat.rasterize(gt, cam)
+    state = lonlat.LonlatState(P, W, H, n0 + n0 // 8 + 4096, dev)
+    img = torch.empty(3, H, W, device=dev)
+    radii = torch.empty(P, dtype=torch.int32, device=dev)
+    grads = lonlat.Gradients.empty(P, 16, dev)
+
+    def plain():
+        state.forward(gt, cam, img, radii)
+        state.backward(gt, cam, radii, dpix, grads)
+
+    out["fp32_plain_ms_per_view"] = _time_steps(plain, args, dev)
+    del state, grads
+    torch.cuda.empty_cache()
+    # precision mode through the batched path
+    gb = lonlat.GaussianTensors(means3D=gt.means3D, opacities=gt.opacities, shs=gt.shs.to(torch.bfloat16),
+                                scales=gt.scales, rotations=gt.rotations)
+    cams = batch.BatchCameras.from_views([view], dev)
+    _, per, sizing = batch.render_batch(gb, cams, fp64_poles=True)
+    del sizing
+    bstate = batch.BatchState(P, cams.sizes, per[0] + per[0] // 8 + 4096, dev)
+    bgr = batch.BatchGradients.empty(P, 16, dev)
+
+    def prec():
+        bstate.forward(gb, cams, [img], fp64_poles=True)
+        bstate.backward(gb, cams, [dpix], bgr, fp64_poles=True)
+
+    out["precision_ms_per_view"] = _time_steps(prec, args, dev)
+    out["num_rendered"] = int(n0)
+    out["workload"] = "6M Gaussians (30% beyond 80 deg latitude), one 4096x2048 view, fwd+bwd"
+    del bstate, bgr, gt, gb
+    torch.cuda.empty_cache()
+    return out
+
+
+def run_peak_memory(dev):
+    """Peak device memory of one fwd+bwd at 4096x2048 over 3M Gaussians through the plain path
+    (transmittance is recomputed in the backward: per pixel only final T and the last-contributor
+    index are stored)."""
+    import torch
+
+    from omnigs_b200 import lonlat, scenes
+
+    P, W, H = 3_000_000, 4096, 2048
+    g = scenes.make_gaussians(P, seed=3)
+    gt = lonlat.GaussianTensors.from_numpy(g, dev)
+    cam = lonlat.Camera.from_view(scenes.identity_view(W, H), dev)
+    dpix = torch.from_numpy(scenes.upstream_grad(W, H, seed=3)).to(dev)
+    torch.cuda.synchronize()
+    base = torch.cuda.memory_allocated(dev)
+    torch.cuda.reset_peak_memory_stats(dev)
+    img, radii, n, state = lonlat.rasterize(gt, cam, capacity=1)  # exact sizing (one resize)
+    grads = lonlat.Gradients.empty(P, 16, dev)
+    state.backward(gt, cam, radii, dpix, grads, R=n)
+    torch.cuda.synchronize()
+    peak = torch.cuda.max_memory_allocated(dev) - base
+    per_pixel_state = 8 * W * H
+    out = {"workload": "3M Gaussians, one 4096x2048 view, fwd+bwd (plain path)", "num_rendered": int(n),
+           "peak_bytes_above_inputs": int(peak), "peak_gb": round(peak / 1e9, 3),
+           "per_pixel_state_bytes": per_pixel_state}
+    del state, grads, img, gt
+    torch.cuda.empty_cache()
+    return out
+
+
+def _time_steps(fn, args, dev):
+    import torch
+
+    for _ in range(max(1, args.warmup)):
+        fn()
+    torch.cuda.synchronize()
+    cur = torch.cuda.current_stream(dev)
+    e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+    k = max(2, args.steps // 4)
+    e0.record(cur)
+    for _ in range(k):
+        fn()
+    e1.record(cur)
+    torch.cuda.synchronize()
+    return round(e0.elapsed_time(e1) / k, 4)
 
 
 # ---------------------------------------------------------------- omnigs arm --------------------
@@ -452,8 +590,11 @@ def run_omnigs(args, rank, world, local_rank):
                "api": "RasterizeGaussiansCUDA + RasterizeGaussiansBackwardCUDA (LibTorch layer)"}
 
     batched = None
+    extra = None
     if world == 1 and not args.no_batch and (P, W, H) == (P_GAUSS, WIDTH, HEIGHT):
-        batched = run_batched(args, gt, dev, value)
+        batched = run_batched(args, g, gt, dev, value)
+        if not args.no_extra:
+            extra = {"precision": run_precision(args, dev), "peak_memory": run_peak_memory(dev)}
 
     cpu = None
     if rank == 0 and world == 1 and not args.no_cpu_baseline:
@@ -470,7 +611,7 @@ def run_omnigs(args, rank, world, local_rank):
                            "num_rendered": n0, "visible": V, "parallelism": f"dp{world} (views)",
                            "l2": "inputs larger than L2 (SH alone 192 MB > 126 MB), no flush"},
                 "gpu_launches": int(launches), "clocks": clocks.summary(), "roofline": roofline,
-                "roofline_fp32": roofline_fp32, "kernels": kernels, "e2e": e2e, "batched": batched,
+                "roofline_fp32": roofline_fp32, "kernels": kernels, "e2e": e2e, "batched": batched, "configs": extra,
                 "cpu_baseline": cpu}
         print(json.dumps(line), flush=True)
 
