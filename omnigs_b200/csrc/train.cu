@@ -9,7 +9,7 @@
 //   dSSIM/dimg(p) = 1/N [ (w * A)(p) + 2 img(p) (w * B)(p) + gt(p) (w * Cm)(p) ]
 // with per-pixel A = dS/dmu1, B = dS/d(w * img^2), Cm = dS/d(w * img gt) (the window is
 // symmetric, so the adjoint convolution is the same convolution).  Kernel 1 computes the local
-// statistics, S and A, B, Cm (written to a workspace) and the two sums (FP64 atomics); kernel 2
+// statistics, S and A, B, Cm (written to a workspace) and per-block FP64 sums; kernel 2
 // convolves A, B, Cm back and writes dL/dimg; kernel 3 writes the three loss values.
 //
 // Adam (torch::optim::Adam as configured at src/gaussian_model.cpp:485-518: per-group learning
@@ -19,6 +19,7 @@
 // backward (exp, sigmoid, L2 normalisation, SH split) is fused into the step, and the kernel
 // writes the activated values for the next forward (SH as FP32 or BF16).  The step counter and
 // learning rates are read from device memory, so a captured CUDA graph replays across steps.
+#include <algorithm>
 #include <cmath>
 #include <cuda_bf16.h>
 
@@ -39,7 +40,7 @@ struct LossParams {
   const float* gt;
   float* dimg;        // [C][H][W] gradient; rows >= `rows` are set to 0
   float* ws;          // [3][C][rows][W]: A, B, Cm
-  double* sums;       // [2]: sum |img - gt|, sum S
+  double* sums;       // [2 * blocks]: per-block sum |img - gt|, sum S
   float* loss;        // [3]: loss, l1, ssim
   int C, H, W, rows;
   float lambda;
@@ -47,50 +48,74 @@ struct LossParams {
 };
 
 // Separable 11-tap convolution with zero padding of a [rows][W] plane region into the tile at
-// (x0, y0); `src(y, x)` gives the input (0 outside [0, rows) x [0, W)).  tmp holds the horizontal
-// pass over the tile's rows plus the halo.
+// (x0, y0); `src(ok, y, x, v)` gives the NQ inputs at (y, x) (zeros when !ok, i.e. outside
+// [0, rows) x [0, W)), `out(y, x, v)` receives the NQ convolved values of an output pixel.  Each
+// pass slides an 11-tap window along a register segment (kSeg outputs from kSeg + 10 loads), so
+// shared memory is read ~1.8 times per output instead of 11 times.
+constexpr int kSeg = 8;
 template <int NQ, class Src, class Out>
 __device__ __forceinline__ void conv_tile(int x0, int y0, int rows, int W, const float* w,
                                           float (*in)[kLossTileH + 2 * kHalf][kLossTileW + 2 * kHalf],
                                           float (*tmp)[kLossTileH + 2 * kHalf][kLossTileW], Src src, Out out) {
   constexpr int IH = kLossTileH + 2 * kHalf, IW = kLossTileW + 2 * kHalf;
-  for (int i = threadIdx.x; i < IH * IW; i += blockDim.x) {
-    const int ty = i / IW, tx = i - ty * IW;
-    const int y = y0 + ty - kHalf, x = x0 + tx - kHalf;
-    const bool ok = y >= 0 && y < rows && x >= 0 && x < W;
-    float v[NQ];
-    src(ok, y, x, v);
+  constexpr int kRowsPerPass = kLossThreads / kLossTileW;  // 8 rows of 32 threads
+  const int lx = threadIdx.x % kLossTileW, ly = threadIdx.x / kLossTileW;
+  for (int ty = ly; ty < IH; ty += kRowsPerPass) {
+    for (int tx = lx; tx < IW; tx += kLossTileW) {
+      const int y = y0 + ty - kHalf, x = x0 + tx - kHalf;
+      const bool ok = y >= 0 && y < rows && x >= 0 && x < W;
+      float v[NQ];
+      src(ok, y, x, v);
 #pragma unroll
-    for (int q = 0; q < NQ; ++q) in[q][ty][tx] = v[q];
-  }
-  __syncthreads();
-  for (int i = threadIdx.x; i < IH * kLossTileW; i += blockDim.x) {
-    const int ty = i / kLossTileW, tx = i - ty * kLossTileW;
-#pragma unroll
-    for (int q = 0; q < NQ; ++q) {
-      float acc = 0.f;
-#pragma unroll
-      for (int k = 0; k < kWin; ++k) acc = fmaf(w[k], in[q][ty][tx + k], acc);
-      tmp[q][ty][tx] = acc;
+      for (int q = 0; q < NQ; ++q) in[q][ty][tx] = v[q];
     }
   }
   __syncthreads();
-  for (int i = threadIdx.x; i < kLossTileH * kLossTileW; i += blockDim.x) {
-    const int ty = i / kLossTileW, tx = i - ty * kLossTileW;
-    float v[NQ];
+  // horizontal: task = (q, row, segment of kSeg output columns)
+  constexpr int kHSegs = kLossTileW / kSeg;
+  for (int t = threadIdx.x; t < NQ * IH * kHSegs; t += kLossThreads) {
+    const int q = t / (IH * kHSegs), rem = t - q * (IH * kHSegs);
+    const int ty = rem / kHSegs, xs = (rem - ty * kHSegs) * kSeg;
+    float r[kSeg + kWin - 1];
 #pragma unroll
-    for (int q = 0; q < NQ; ++q) {
+    for (int k = 0; k < kSeg + kWin - 1; ++k) r[k] = in[q][ty][xs + k];
+#pragma unroll
+    for (int j = 0; j < kSeg; ++j) {
       float acc = 0.f;
 #pragma unroll
-      for (int k = 0; k < kWin; ++k) acc = fmaf(w[k], tmp[q][ty + k][tx], acc);
-      v[q] = acc;
+      for (int k = 0; k < kWin; ++k) acc = fmaf(w[k], r[j + k], acc);
+      tmp[q][ty][xs + j] = acc;
     }
-    const int y = y0 + ty, x = x0 + tx;
+  }
+  __syncthreads();
+  // vertical: task = (q, column, segment of kSeg output rows); results reuse `in`
+  constexpr int kVSegs = kLossTileH / kSeg;
+  for (int t = threadIdx.x; t < NQ * kLossTileW * kVSegs; t += kLossThreads) {
+    const int q = t / (kLossTileW * kVSegs), rem = t - q * (kLossTileW * kVSegs);
+    const int ys = (rem / kLossTileW) * kSeg, tx = rem % kLossTileW;
+    float r[kSeg + kWin - 1];
+#pragma unroll
+    for (int k = 0; k < kSeg + kWin - 1; ++k) r[k] = tmp[q][ys + k][tx];
+#pragma unroll
+    for (int j = 0; j < kSeg; ++j) {
+      float acc = 0.f;
+#pragma unroll
+      for (int k = 0; k < kWin; ++k) acc = fmaf(w[k], r[j + k], acc);
+      in[q][ys + j][tx] = acc;
+    }
+  }
+  __syncthreads();
+  for (int ty = ly; ty < kLossTileH; ty += kRowsPerPass) {
+    float v[NQ];
+#pragma unroll
+    for (int q = 0; q < NQ; ++q) v[q] = in[q][ty][lx];
+    const int y = y0 + ty, x = x0 + lx;
     if (y < rows && x < W) out(y, x, v);
   }
 }
 
-__device__ __forceinline__ void block_add2(double a, double b, double* sums) {
+// Block sums of (a, b) into partials[2 * block] (no contended atomics; loss_finalize adds them).
+__device__ __forceinline__ void block_sum2(double a, double b, double* partials) {
   __shared__ double s_red[2][kLossThreads / 32];
   const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
 #pragma unroll
@@ -109,8 +134,9 @@ __device__ __forceinline__ void block_add2(double a, double b, double* sums) {
       ta += s_red[0][k];
       tb += s_red[1][k];
     }
-    atomicAdd(&sums[0], ta);
-    atomicAdd(&sums[1], tb);
+    const size_t blk = ((size_t)blockIdx.z * gridDim.y + blockIdx.y) * gridDim.x + blockIdx.x;
+    partials[2 * blk] = ta;
+    partials[2 * blk + 1] = tb;
   }
 }
 
@@ -155,7 +181,7 @@ __global__ void __launch_bounds__(kLossThreads) ssim_stats_kernel(const __grid_c
     l1 += (double)fabsf(a[o] - b[o]);
   };
   conv_tile<5>(x0, y0, p.rows, p.W, p.w, s_in, s_tmp, src, out);
-  block_add2(l1, ssum, p.sums);
+  block_sum2(l1, ssum, p.sums);
 }
 
 // Kernel 2: dL/dimg of one tile of one channel.
@@ -199,11 +225,36 @@ __global__ void __launch_bounds__(kLossThreads) ssim_grad_kernel(const __grid_co
   }
 }
 
-__global__ void loss_finalize_kernel(const double* sums, float* loss, double invN, float lambda) {
-  const double l1 = sums[0] * invN, ssim = sums[1] * invN;
-  loss[0] = (float)((1.0 - lambda) * l1 + lambda * (1.0 - ssim));
-  loss[1] = (float)l1;
-  loss[2] = (float)ssim;
+__global__ void __launch_bounds__(1024) loss_finalize_kernel(const double* partials, int blocks, float* loss,
+                                                              double invN, float lambda) {
+  __shared__ double s_red[2][32];
+  double a = 0.0, b = 0.0;
+  for (int i = threadIdx.x; i < blocks; i += blockDim.x) {
+    a += partials[2 * i];
+    b += partials[2 * i + 1];
+  }
+  const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
+#pragma unroll
+  for (int o = 16; o > 0; o >>= 1) {
+    a += __shfl_xor_sync(kFullMask, a, o);
+    b += __shfl_xor_sync(kFullMask, b, o);
+  }
+  if (lane == 0) {
+    s_red[0][warp] = a;
+    s_red[1][warp] = b;
+  }
+  __syncthreads();
+  if (threadIdx.x == 0) {
+    double ta = 0.0, tb = 0.0;
+    for (int k = 0; k < (int)(blockDim.x / 32); ++k) {
+      ta += s_red[0][k];
+      tb += s_red[1][k];
+    }
+    const double l1 = ta * invN, ssim = tb * invN;
+    loss[0] = (float)((1.0 - lambda) * l1 + lambda * (1.0 - ssim));
+    loss[1] = (float)l1;
+    loss[2] = (float)ssim;
+  }
 }
 
 // ---------------------------------------------------------------- Adam ------------------------
@@ -249,14 +300,18 @@ __device__ __forceinline__ float adam_update(float& p, float& m, float& v, float
 }
 
 __global__ void __launch_bounds__(256) adam_gaussian_kernel(const __grid_constant__ AdamParams p) {
+  __shared__ AdamScalars s_sc[6];
   const int P = p.prm.P, M = p.prm.M;
   const int64_t rest_n = (int64_t)P * (M - 1) * 3;
-  const int64_t i = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
-  const OmnigsAdamHyper h = *p.hyper;
+  if (threadIdx.x < 6) s_sc[threadIdx.x] = adam_scalars(*p.hyper, threadIdx.x);
+  __syncthreads();
+  // grid-stride over [0, P) (per-Gaussian groups) and [P, P + rest_n) (f_rest elements)
+  for (int64_t i = (int64_t)blockIdx.x * blockDim.x + threadIdx.x; i < P + rest_n;
+       i += (int64_t)gridDim.x * blockDim.x) {
   if (i < P) {
     const int g = (int)i;
     {  // xyz (group 0): the activated mean is the parameter itself
-      const AdamScalars s = adam_scalars(h, 0);
+      const AdamScalars& s = s_sc[0];
       for (int k = 0; k < 3; ++k) {
         const float v = adam_update(p.prm.xyz[3 * g + k], p.st.m_xyz[3 * g + k], p.st.v_xyz[3 * g + k],
                                     p.dL_dmeans3D[3 * g + k], s);
@@ -264,7 +319,7 @@ __global__ void __launch_bounds__(256) adam_gaussian_kernel(const __grid_constan
       }
     }
     {  // f_dc (group 1) = SH coefficient 0
-      const AdamScalars s = adam_scalars(h, 1);
+      const AdamScalars& s = s_sc[1];
       for (int k = 0; k < 3; ++k) {
         const float v = adam_update(p.prm.features_dc[3 * g + k], p.st.m_dc[3 * g + k], p.st.v_dc[3 * g + k],
                                     p.dL_dsh[(size_t)g * M * 3 + k], s);
@@ -275,14 +330,14 @@ __global__ void __launch_bounds__(256) adam_gaussian_kernel(const __grid_constan
       }
     }
     {  // opacity (group 3), sigmoid
-      const AdamScalars s = adam_scalars(h, 3);
+      const AdamScalars& s = s_sc[3];
       const float o = p.act.opacities[g];  // sigmoid of the current parameter (previous forward)
       const float grad = p.dL_dopacity[g] * o * (1.f - o);
       const float v = adam_update(p.prm.opacity[g], p.st.m_opacity[g], p.st.v_opacity[g], grad, s);
       p.act.opacities[g] = 1.f / (1.f + expf(-v));
     }
     {  // scaling (group 4), exp
-      const AdamScalars s = adam_scalars(h, 4);
+      const AdamScalars& s = s_sc[4];
       for (int k = 0; k < 3; ++k) {
         const float e = p.act.scales[3 * g + k];  // exp of the current parameter
         const float v = adam_update(p.prm.scaling[3 * g + k], p.st.m_scaling[3 * g + k], p.st.v_scaling[3 * g + k],
@@ -291,7 +346,7 @@ __global__ void __launch_bounds__(256) adam_gaussian_kernel(const __grid_constan
       }
     }
     {  // rotation (group 5), L2 normalisation (F.normalize, eps 1e-12)
-      const AdamScalars s = adam_scalars(h, 5);
+      const AdamScalars& s = s_sc[5];
       float r[4], gr[4];
       for (int k = 0; k < 4; ++k) {
         r[k] = p.prm.rotation[4 * g + k];
@@ -308,18 +363,20 @@ __global__ void __launch_bounds__(256) adam_gaussian_kernel(const __grid_constan
       const float n2 = fmaxf(sqrtf(nr[0] * nr[0] + nr[1] * nr[1] + nr[2] * nr[2] + nr[3] * nr[3]), 1e-12f);
       for (int k = 0; k < 4; ++k) p.act.rotations[4 * g + k] = nr[k] / n2;
     }
-  } else if (i - P < rest_n) {
+  } else {
     // f_rest (group 2), elementwise: element e of Gaussian g's (M - 1) x 3 rest coefficients
-    const int64_t e = i - P;
-    const int64_t per = (int64_t)(M - 1) * 3;
-    const int64_t g = e / per, r = e - g * per;
-    const AdamScalars s = adam_scalars(h, 2);
+    // (rest_n < 2^32 is checked on the host, so 32-bit index arithmetic suffices)
+    const uint32_t e = (uint32_t)(i - P);
+    const uint32_t per = (uint32_t)(M - 1) * 3u;
+    const uint32_t g = e / per, r = e - g * per;
+    const AdamScalars& s = s_sc[2];
     const size_t sh_idx = (size_t)g * M * 3 + 3 + r;
     const float v = adam_update(p.prm.features_rest[e], p.st.m_rest[e], p.st.v_rest[e], p.dL_dsh[sh_idx], s);
     if (p.act.shs_bf16)
       reinterpret_cast<__nv_bfloat16*>(p.act.shs)[sh_idx] = __float2bfloat16_rn(v);
     else
       static_cast<float*>(p.act.shs)[sh_idx] = v;
+  }
   }
 }
 
@@ -347,9 +404,9 @@ __global__ void __launch_bounds__(256) activate_kernel(const OmnigsGaussianParam
     const float n = fmaxf(sqrtf(r[0] * r[0] + r[1] * r[1] + r[2] * r[2] + r[3] * r[3]), 1e-12f);
     for (int k = 0; k < 4; ++k) act.rotations[4 * g + k] = r[k] / n;
   } else if (i - P < rest_n) {
-    const int64_t e = i - P;
-    const int64_t per = (int64_t)(M - 1) * 3;
-    const int64_t g = e / per, r = e - g * per;
+    const uint32_t e = (uint32_t)(i - P);
+    const uint32_t per = (uint32_t)(M - 1) * 3u;
+    const uint32_t g = e / per, r = e - g * per;
     put_sh((size_t)g * M * 3 + 3 + r, prm.features_rest[e]);
   }
 }
@@ -358,6 +415,8 @@ int validate_params(const OmnigsGaussianParams* prm, const OmnigsActivated* act)
   if (prm == nullptr || act == nullptr) return fail(OMNIGS_ERR_INVALID_ARGUMENT, "parameters are NULL");
   if (prm->P < 0 || prm->M < 1 || prm->M > 16)
     return fail(OMNIGS_ERR_INVALID_ARGUMENT, "P must be >= 0 and M (SH coefficients) in [1, 16]");
+  if ((int64_t)prm->P * (prm->M - 1) * 3 >= (int64_t(1) << 32))
+    return fail(OMNIGS_ERR_INVALID_ARGUMENT, "P * (M - 1) * 3 must be below 2^32");
   if (prm->P == 0) return OMNIGS_OK;
   if (!prm->xyz || !prm->features_dc || (prm->M > 1 && !prm->features_rest) || !prm->opacity || !prm->scaling ||
       !prm->rotation || !act->means3D || !act->shs || !act->opacities || !act->scales || !act->rotations)
@@ -374,7 +433,8 @@ extern "C" {
 
 size_t omnigs_l1_dssim_workspace_bytes(int C, int H, int W) {
   if (C <= 0 || H <= 0 || W <= 0) return 0;
-  return align_up(sizeof(double) * 2) + sizeof(float) * 3 * (size_t)C * H * W;
+  const size_t blocks = (size_t)C * ((W + kLossTileW - 1) / kLossTileW) * ((H + kLossTileH - 1) / kLossTileH);
+  return align_up(sizeof(double) * 2 * blocks) + sizeof(float) * 3 * (size_t)C * H * W;
 }
 
 int omnigs_l1_dssim(const float* image, const float* gt, int C, int H, int W, int rows, float lambda_dssim,
@@ -393,8 +453,10 @@ int omnigs_l1_dssim(const float* image, const float* gt, int C, int H, int W, in
   p.img = image;
   p.gt = gt;
   p.dimg = dL_dimage;
+  const dim3 grid((W + kLossTileW - 1) / kLossTileW, (rows + kLossTileH - 1) / kLossTileH, C);
+  const size_t max_blocks = (size_t)C * ((W + kLossTileW - 1) / kLossTileW) * ((H + kLossTileH - 1) / kLossTileH);
   p.sums = static_cast<double*>(workspace);
-  p.ws = reinterpret_cast<float*>(static_cast<unsigned char*>(workspace) + align_up(sizeof(double) * 2));
+  p.ws = reinterpret_cast<float*>(static_cast<unsigned char*>(workspace) + align_up(sizeof(double) * 2 * max_blocks));
   p.loss = loss;
   p.C = C;
   p.H = H;
@@ -409,12 +471,11 @@ int omnigs_l1_dssim(const float* image, const float* gt, int C, int H, int W, in
     sum += p.w[k];
   }
   for (int k = 0; k < kWin; ++k) p.w[k] /= sum;
-  if (cudaMemsetAsync(p.sums, 0, sizeof(double) * 2, s) != cudaSuccess) return check_launch("memset loss sums");
-  const dim3 grid((W + kLossTileW - 1) / kLossTileW, (rows + kLossTileH - 1) / kLossTileH, C);
+  const int blocks = (int)(grid.x * grid.y * grid.z);
   staged(OMNIGS_STAGE_OTHER, 3, s, [&] {
     ssim_stats_kernel<<<grid, kLossThreads, 0, s>>>(p);
     ssim_grad_kernel<<<grid, kLossThreads, 0, s>>>(p);
-    loss_finalize_kernel<<<1, 1, 0, s>>>(p.sums, loss, 1.0 / ((double)C * rows * W), lambda_dssim);
+    loss_finalize_kernel<<<1, 1024, 0, s>>>(p.sums, blocks, loss, 1.0 / ((double)C * rows * W), lambda_dssim);
   });
   return check_launch("l1 + d-ssim");
 }
@@ -453,8 +514,11 @@ int omnigs_adam_step(const OmnigsGaussianParams* prm, const OmnigsAdamState* st,
   p.dL_drotations = dL_drotations;
   p.hyper = hyper;
   const int64_t n = (int64_t)prm->P + (int64_t)prm->P * (prm->M - 1) * 3;
-  staged(OMNIGS_STAGE_OTHER, 1, s,
-         [&] { adam_gaussian_kernel<<<(unsigned)((n + 255) / 256), 256, 0, s>>>(p); });
+  int dev = 0, sms = 148;
+  cudaGetDevice(&dev);
+  cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev);
+  const unsigned blocks = (unsigned)std::min<int64_t>((n + 255) / 256, (int64_t)sms * 8);
+  staged(OMNIGS_STAGE_OTHER, 1, s, [&] { adam_gaussian_kernel<<<blocks, 256, 0, s>>>(p); });
   return check_launch("adam step");
 }
 
