@@ -249,6 +249,28 @@ int omnigs_batch_backward(const OmnigsBatchArgs* args, const OmnigsBatchGrads* g
                           size_t state_bytes, const void* binning, size_t binning_bytes,
                           omnigs_stream_t stream);
 
+/* Splats staged per shared-memory batch in the blend kernels, per direction: 128, 256 (default)
+ * or 512.  Results do not depend on it (every pixel meets the same splats in the same order);
+ * the best size depends on the scene and resolution.  Process-wide setting. */
+int omnigs_set_blend_batch(int forward, int backward);
+int omnigs_get_blend_batch(int* forward, int* backward);
+
+/* Autotuner of the blend staging batch: on a batch whose forward has completed (state and
+ * binning hold the sorted instance lists; every view needs out_color and dL_dout_color), times
+ * the forward and backward blends of all views for each candidate size (`repeats` timed launches
+ * each, CUDA events on `stream`), selects the fastest per direction with omnigs_set_blend_batch
+ * and reports the times.  It synchronises the host.  The forward outputs are rewritten with
+ * identical values and the gradient accumulators are cleared, so omnigs_batch_backward may follow
+ * directly. */
+typedef struct OmnigsTuneResult {
+  int candidates[3];
+  float forward_ms[3];
+  float backward_ms[3];
+  int forward_batch, backward_batch;
+} OmnigsTuneResult;
+int omnigs_batch_autotune(const OmnigsBatchArgs* args, void* state, size_t state_bytes, void* binning,
+                          size_t binning_bytes, int repeats, OmnigsTuneResult* out, omnigs_stream_t stream);
+
 /* Waits for `stream`; returns the total instance count, the per-view counts (view_rendered[V], may
  * be NULL) and the status word. */
 int omnigs_batch_read_status(const void* state, int V, int64_t* num_rendered, int64_t* view_rendered,

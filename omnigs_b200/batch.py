@@ -148,6 +148,20 @@ class BatchState:
                                               self.binning.numel(), capi.stream_handle(stream))
         capi.check(rc, "omnigs_batch_backward")
 
+    def autotune(self, g: GaussianTensors, cams: BatchCameras, images, dL_dimages, D: int = 3,
+                 scale_modifier: float = 1.0, fp64_poles: bool = False, repeats: int = 3, stream=None) -> dict:
+        """Chooses the blend staging batch (128 / 256 / 512 splats) per direction by timing the
+        blends of this batch; needs a completed forward.  Synchronises; process-wide setting."""
+        a, keep = self._args(g, cams, images, dL_dimages, D, scale_modifier, fp64_poles)
+        r = capi.TuneResult()
+        rc = capi.lib().omnigs_batch_autotune(ctypes.byref(a), self.state.data_ptr(), self.state.numel(),
+                                              self.binning.data_ptr(), self.binning.numel(), repeats,
+                                              ctypes.byref(r), capi.stream_handle(stream))
+        capi.check(rc, "omnigs_batch_autotune")
+        return {"candidates": list(r.candidates), "forward_ms": [round(x, 4) for x in r.forward_ms],
+                "backward_ms": [round(x, 4) for x in r.backward_ms], "forward_batch": r.forward_batch,
+                "backward_batch": r.backward_batch}
+
     def status(self, stream=None) -> tuple[int, list, int]:
         """(total instances, instances per view, status bits); synchronises the stream."""
         n = ctypes.c_int64(0)
@@ -184,6 +198,17 @@ class BatchState:
             out["tile_base"].append(int(tb))
             out["pixel_base"].append(int(pb))
         return out
+
+
+def set_blend_batch(forward: int, backward: int):
+    """Splats staged per shared-memory batch in the blend kernels (128, 256 or 512 each)."""
+    capi.check(capi.lib().omnigs_set_blend_batch(forward, backward), "omnigs_set_blend_batch")
+
+
+def get_blend_batch() -> tuple[int, int]:
+    f, b = ctypes.c_int(0), ctypes.c_int(0)
+    capi.lib().omnigs_get_blend_batch(ctypes.byref(f), ctypes.byref(b))
+    return int(f.value), int(b.value)
 
 
 def render_batch(g: GaussianTensors, cams: BatchCameras, D: int = 3, scale_modifier: float = 1.0,

@@ -117,6 +117,11 @@ class AdamHyper(ctypes.Structure):
                 ("eps", ctypes.c_double), ("step", ctypes.c_int64)]
 
 
+class TuneResult(ctypes.Structure):
+    _fields_ = [("candidates", _i * 3), ("forward_ms", _f * 3), ("backward_ms", _f * 3),
+                ("forward_batch", _i), ("backward_batch", _i)]
+
+
 # every symbol include/omnigs_b200.h declares
 EXPORTED = ["omnigs_version", "omnigs_last_error", "omnigs_lonlat_geom_bytes",
             "omnigs_lonlat_image_bytes", "omnigs_lonlat_binning_bytes",
@@ -128,7 +133,8 @@ EXPORTED = ["omnigs_version", "omnigs_last_error", "omnigs_lonlat_geom_bytes",
             "omnigs_lonlat_image_view", "omnigs_batch_state_bytes", "omnigs_batch_forward",
             "omnigs_batch_render", "omnigs_batch_backward", "omnigs_batch_read_status",
             "omnigs_batch_state_view", "omnigs_l1_dssim_workspace_bytes", "omnigs_l1_dssim",
-            "omnigs_activate", "omnigs_adam_step"]
+            "omnigs_activate", "omnigs_adam_step", "omnigs_set_blend_batch", "omnigs_get_blend_batch",
+            "omnigs_batch_autotune"]
 
 _lib = None
 
@@ -182,6 +188,10 @@ def lib() -> ctypes.CDLL:
         L.omnigs_l1_dssim_workspace_bytes.restype = ctypes.c_size_t
         L.omnigs_l1_dssim_workspace_bytes.argtypes = [_i, _i, _i]
         L.omnigs_l1_dssim.argtypes = [_vp, _vp, _i, _i, _i, _i, _f, _vp, _vp, _vp, ctypes.c_size_t, _vp]
+        L.omnigs_set_blend_batch.argtypes = [_i, _i]
+        L.omnigs_get_blend_batch.argtypes = [ctypes.POINTER(_i), ctypes.POINTER(_i)]
+        L.omnigs_batch_autotune.argtypes = [ctypes.POINTER(BatchArgs), _vp, ctypes.c_size_t, _vp, ctypes.c_size_t,
+                                            _i, ctypes.POINTER(TuneResult), _vp]
         L.omnigs_activate.argtypes = [ctypes.POINTER(GaussianParams), ctypes.POINTER(Activated), _vp]
         L.omnigs_adam_step.argtypes = [ctypes.POINTER(GaussianParams), ctypes.POINTER(AdamState),
                                        ctypes.POINTER(Activated), _vp, _vp, _vp, _vp, _vp, _vp, _vp]

@@ -372,6 +372,85 @@ int omnigs_batch_backward(const OmnigsBatchArgs* a, const OmnigsBatchGrads* g, v
   return check_launch("batch preprocess backward");
 }
 
+int omnigs_batch_autotune(const OmnigsBatchArgs* a, void* state, size_t state_bytes, void* binning,
+                          size_t binning_bytes, int repeats, OmnigsTuneResult* out, omnigs_stream_t stream) {
+  g_last_error.clear();
+  BatchPlan plan;
+  if (int rc = validate_batch(a, plan)) return rc;
+  if (out == nullptr || repeats < 1) return fail(OMNIGS_ERR_INVALID_ARGUMENT, "out is NULL or repeats < 1");
+  for (int v = 0; v < a->V; ++v)
+    if (a->views[v].out_color == nullptr || a->views[v].dL_dout_color == nullptr)
+      return fail(OMNIGS_ERR_INVALID_ARGUMENT, "every view needs out_color and dL_dout_color");
+  const int cand[3] = {128, 256, 512};
+  std::memset(out, 0, sizeof(*out));
+  for (int k = 0; k < 3; ++k) out->candidates[k] = cand[k];
+  out->forward_batch = g_blend_batch[0].load();
+  out->backward_batch = g_blend_batch[1].load();
+  if (a->P == 0) return OMNIGS_OK;
+  const BatchLayout L = batch_layout(a->P, plan);
+  if (int rc = check_state(L, state, state_bytes)) return rc;
+  int64_t capacity = BinningLayout::capacity_for(binning_bytes);
+  if (binning == nullptr || capacity < 0)
+    return fail(OMNIGS_ERR_BUFFER_TOO_SMALL, "binning buffer smaller than omnigs_lonlat_binning_bytes(0)");
+  const BinningLayout BL = BinningLayout::make(capacity);
+  if (capacity > kMaxInstances) capacity = kMaxInstances;
+  cudaStream_t s = reinterpret_cast<cudaStream_t>(stream);
+  GeomHeader h;
+  if (cudaMemcpyAsync(&h, state, sizeof(h), cudaMemcpyDeviceToHost, s) != cudaSuccess ||
+      cudaStreamSynchronize(s) != cudaSuccess)
+    return check_launch("read batch status");
+  if (h.status != 0)
+    return fail(OMNIGS_ERR_DEVICE, "the batch state holds no complete forward (status word set); run omnigs_batch_forward first");
+  const int fin = TileDigits::from_tiles((uint32_t)plan.tiles).passes & 1;
+  const BatchParams bp = batch_params(a, plan, state, L);
+  const BatchRenderParams r =
+      render_params(bp, plan, state, L, at<uint32_t>(binning, fin ? BL.tvals1 : BL.tvals0), capacity);
+  cudaEvent_t e0 = nullptr, e1 = nullptr;
+  if (cudaEventCreate(&e0) != cudaSuccess || cudaEventCreate(&e1) != cudaSuccess) return check_launch("events");
+  const int saved[2] = {g_blend_batch[0].load(), g_blend_batch[1].load()};
+  int rc = OMNIGS_OK;
+  for (int dir = 0; dir < 2 && rc == OMNIGS_OK; ++dir) {
+    float best = 0.f;
+    int best_b = saved[dir];
+    for (int k = 0; k < 3; ++k) {
+      g_blend_batch[dir].store(cand[k]);
+      auto launch = [&] {
+        if (dir == 0)
+          launch_batch_render_forward(r, s);
+        else
+          launch_batch_render_backward(r, s);
+        g_launches.fetch_add(1, std::memory_order_relaxed);
+      };
+      launch();  // warm-up
+      cudaEventRecord(e0, s);
+      for (int t = 0; t < repeats; ++t) launch();
+      cudaEventRecord(e1, s);
+      float ms = 0.f;
+      if (cudaEventSynchronize(e1) != cudaSuccess || cudaEventElapsedTime(&ms, e0, e1) != cudaSuccess) {
+        rc = check_launch("autotune timing");
+        break;
+      }
+      ms /= repeats;
+      (dir == 0 ? out->forward_ms : out->backward_ms)[k] = ms;
+      if (k == 0 || ms < best) {
+        best = ms;
+        best_b = cand[k];
+      }
+    }
+    g_blend_batch[dir].store(rc == OMNIGS_OK ? best_b : saved[dir]);
+  }
+  cudaEventDestroy(e0);
+  cudaEventDestroy(e1);
+  if (rc) return rc;
+  out->forward_batch = g_blend_batch[0].load();
+  out->backward_batch = g_blend_batch[1].load();
+  // the timed backward launches summed into the accumulators: clear them for the real backward
+  if (cudaMemsetAsync(at<unsigned char>(state, L.grad_acc), 0, sizeof(float) * 12 * (size_t)a->P * a->V, s) !=
+      cudaSuccess)
+    return check_launch("clear accumulators");
+  return check_launch("autotune");
+}
+
 int omnigs_batch_read_status(const void* state, int V, int64_t* num_rendered, int64_t* view_rendered,
                              uint32_t* status, omnigs_stream_t stream) {
   g_last_error.clear();

@@ -7,8 +7,6 @@
 
 namespace omnigs {
 
-// Splats staged per shared-memory batch.
-constexpr int kBatch = 256;
 // Pixels per thread: a thread owns kBlendPx pixels of one column, 4 rows apart, so a warp (8
 // columns x 4 rows of threads) owns an 8 x (4 kBlendPx) patch and a block of kBlendThreads
 // threads one 16x16 tile.

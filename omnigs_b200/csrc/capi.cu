@@ -114,6 +114,9 @@ __global__ void mark_visible_kernel(int P, const float* means3D, const float* vm
 
 void set_last_error(const char* msg) { g_last_error = msg; }
 
+std::atomic<int> g_blend_batch[2] = {{kDefaultBatch}, {kDefaultBatch}};
+int blend_batch_size(bool backward) { return g_blend_batch[backward ? 1 : 0].load(std::memory_order_relaxed); }
+
 void launch_mark_visible(int P, const float* means3D, const float* viewmatrix, int camera_type,
                          bool* present, cudaStream_t s) {
   if (P <= 0) return;
@@ -449,6 +452,21 @@ int omnigs_mark_visible(int P, const float* means3D, const float* viewmatrix, in
     launch_mark_visible(P, means3D, viewmatrix, camera_type, reinterpret_cast<bool*>(present), s);
   });
   return check_launch("mark visible");
+}
+
+int omnigs_set_blend_batch(int forward, int backward) {
+  g_last_error.clear();
+  auto ok = [](int b) { return b == 128 || b == 256 || b == 512; };
+  if (!ok(forward) || !ok(backward)) return fail(OMNIGS_ERR_INVALID_ARGUMENT, "blend batch sizes must be 128, 256 or 512");
+  g_blend_batch[0].store(forward);
+  g_blend_batch[1].store(backward);
+  return OMNIGS_OK;
+}
+
+int omnigs_get_blend_batch(int* forward, int* backward) {
+  if (forward) *forward = g_blend_batch[0].load();
+  if (backward) *backward = g_blend_batch[1].load();
+  return OMNIGS_OK;
 }
 
 int omnigs_timing_enable(int enable) {

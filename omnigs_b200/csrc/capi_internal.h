@@ -64,6 +64,9 @@ void staged(int stage, int kernels, cudaStream_t s, F&& launch) {
   g_timed.push_back(t);
 }
 
+// Blend staging batch size per direction (0 forward, 1 backward), see blend_batch_size.
+extern std::atomic<int> g_blend_batch[2];
+
 // Clears the per-pass state in the header (status capacity bits, counters) and copies the
 // instance total into num_rendered; one thread.
 void launch_begin_render(GeomHeader* hdr, cudaStream_t s);

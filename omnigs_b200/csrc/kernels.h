@@ -217,6 +217,12 @@ void launch_histogram(const HistParams& p, int64_t max_items, cudaStream_t s);
 void launch_onesweep(const OnesweepParams& p, int64_t max_items, cudaStream_t s);
 void launch_duplicate(const DuplicateParams& p, cudaStream_t s);
 void launch_ranges(const RangesParams& p, cudaStream_t s);
+// Splats staged per shared-memory batch in the blend kernels: a template parameter chosen at run
+// time per direction (128, 256 or 512; set by omnigs_set_blend_batch or the autotuner).  Results
+// do not depend on it: every pixel meets the same splats in the same order.
+constexpr int kDefaultBatch = 256;
+int blend_batch_size(bool backward);
+
 void launch_render_forward(const RenderParams& p, cudaStream_t s);
 void launch_render_backward(const RenderParams& p, cudaStream_t s);
 void launch_preprocess_backward(const PreprocessBackwardParams& p, cudaStream_t s);

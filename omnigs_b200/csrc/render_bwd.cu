@@ -59,6 +59,7 @@ __device__ __forceinline__ float rcp_approx(float x) {
   return r;
 }
 
+template <int kBatch>
 __device__ __forceinline__ void blend_backward_tile(const TileJob& job, const BlendSource& src, float* grad_acc) {
   static_assert(kBlendPx == 2, "the backward blend packs a thread's two pixels into f32x2 lanes");
   __shared__ float4 s_a[kBatch];
@@ -197,6 +198,7 @@ __device__ __forceinline__ void blend_backward_tile(const TileJob& job, const Bl
 }
 
 // One view: block (x, y) back-propagates tile (x, y).
+template <int kBatch>
 __global__ void __launch_bounds__(kBlendThreads) render_backward_kernel(RenderParams p) {
   TileJob job;
   job.tile_x = blockIdx.x;
@@ -209,13 +211,14 @@ __global__ void __launch_bounds__(kBlendThreads) render_backward_kernel(RenderPa
   job.final_T = p.final_T;
   job.n_contrib = p.n_contrib;
   job.dL_dpix = p.dL_dpix;
-  blend_backward_tile(job, BlendSource{p.point_list, p.splat, p.color, (uint32_t)p.P, p.capacity}, p.grad_acc);
+  blend_backward_tile<kBatch>(job, BlendSource{p.point_list, p.splat, p.color, (uint32_t)p.P, p.capacity}, p.grad_acc);
 }
 
 // All views of a batch in one launch: block b back-propagates global tile b.
+template <int kBatch>
 __global__ void __launch_bounds__(kBlendThreads) batch_render_backward_kernel(const __grid_constant__ BatchRenderParams p) {
   const TileJob job = batch_tile_job(p, blockIdx.x);
-  blend_backward_tile(job, BlendSource{p.point_list, p.splat, p.color, (uint32_t)p.P * (uint32_t)p.V, p.capacity},
+  blend_backward_tile<kBatch>(job, BlendSource{p.point_list, p.splat, p.color, (uint32_t)p.P * (uint32_t)p.V, p.capacity},
                       p.grad_acc);
 }
 
@@ -223,12 +226,21 @@ __global__ void __launch_bounds__(kBlendThreads) batch_render_backward_kernel(co
 
 void launch_render_backward(const RenderParams& p, cudaStream_t s) {
   if (p.gx <= 0 || p.gy <= 0) return;
-  render_backward_kernel<<<dim3(p.gx, p.gy), kBlendThreads, 0, s>>>(p);
+  const dim3 grid(p.gx, p.gy);
+  switch (blend_batch_size(true)) {
+    case 128: render_backward_kernel<128><<<grid, kBlendThreads, 0, s>>>(p); break;
+    case 512: render_backward_kernel<512><<<grid, kBlendThreads, 0, s>>>(p); break;
+    default: render_backward_kernel<256><<<grid, kBlendThreads, 0, s>>>(p); break;
+  }
 }
 
 void launch_batch_render_backward(const BatchRenderParams& p, cudaStream_t s) {
   if (p.total_tiles == 0) return;
-  batch_render_backward_kernel<<<p.total_tiles, kBlendThreads, 0, s>>>(p);
+  switch (blend_batch_size(true)) {
+    case 128: batch_render_backward_kernel<128><<<p.total_tiles, kBlendThreads, 0, s>>>(p); break;
+    case 512: batch_render_backward_kernel<512><<<p.total_tiles, kBlendThreads, 0, s>>>(p); break;
+    default: batch_render_backward_kernel<256><<<p.total_tiles, kBlendThreads, 0, s>>>(p); break;
+  }
 }
 
 }  // namespace omnigs

@@ -20,6 +20,7 @@
 namespace omnigs {
 namespace {
 
+template <int kBatch>
 __device__ __forceinline__ void blend_forward_tile(const TileJob& job, const BlendSource& src) {
   static_assert(kBlendPx == 2, "the forward blend packs a thread's two pixels into f32x2 lanes");
   __shared__ float4 s_a[kBatch];  // x, y, conic a, conic b
@@ -106,6 +107,7 @@ __device__ __forceinline__ void blend_forward_tile(const TileJob& job, const Ble
 }
 
 // One view: block (x, y) blends tile (x, y).
+template <int kBatch>
 __global__ void __launch_bounds__(kBlendThreads) render_forward_kernel(RenderParams p) {
   TileJob job;
   job.tile_x = blockIdx.x;
@@ -118,25 +120,35 @@ __global__ void __launch_bounds__(kBlendThreads) render_forward_kernel(RenderPar
   job.final_T = p.final_T;
   job.n_contrib = p.n_contrib;
   job.dL_dpix = nullptr;
-  blend_forward_tile(job, BlendSource{p.point_list, p.splat, p.color, (uint32_t)p.P, p.capacity});
+  blend_forward_tile<kBatch>(job, BlendSource{p.point_list, p.splat, p.color, (uint32_t)p.P, p.capacity});
 }
 
 // All views of a batch in one launch: block b blends global tile b.
+template <int kBatch>
 __global__ void __launch_bounds__(kBlendThreads) batch_render_forward_kernel(const __grid_constant__ BatchRenderParams p) {
   const TileJob job = batch_tile_job(p, blockIdx.x);
-  blend_forward_tile(job, BlendSource{p.point_list, p.splat, p.color, (uint32_t)p.P * (uint32_t)p.V, p.capacity});
+  blend_forward_tile<kBatch>(job, BlendSource{p.point_list, p.splat, p.color, (uint32_t)p.P * (uint32_t)p.V, p.capacity});
 }
 
 }  // namespace
 
 void launch_render_forward(const RenderParams& p, cudaStream_t s) {
   if (p.gx <= 0 || p.gy <= 0) return;
-  render_forward_kernel<<<dim3(p.gx, p.gy), kBlendThreads, 0, s>>>(p);
+  const dim3 grid(p.gx, p.gy);
+  switch (blend_batch_size(false)) {
+    case 128: render_forward_kernel<128><<<grid, kBlendThreads, 0, s>>>(p); break;
+    case 512: render_forward_kernel<512><<<grid, kBlendThreads, 0, s>>>(p); break;
+    default: render_forward_kernel<256><<<grid, kBlendThreads, 0, s>>>(p); break;
+  }
 }
 
 void launch_batch_render_forward(const BatchRenderParams& p, cudaStream_t s) {
   if (p.total_tiles == 0) return;
-  batch_render_forward_kernel<<<p.total_tiles, kBlendThreads, 0, s>>>(p);
+  switch (blend_batch_size(false)) {
+    case 128: batch_render_forward_kernel<128><<<p.total_tiles, kBlendThreads, 0, s>>>(p); break;
+    case 512: batch_render_forward_kernel<512><<<p.total_tiles, kBlendThreads, 0, s>>>(p); break;
+    default: batch_render_forward_kernel<256><<<p.total_tiles, kBlendThreads, 0, s>>>(p); break;
+  }
 }
 
 }  // namespace omnigs

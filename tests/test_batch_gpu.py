@@ -164,3 +164,42 @@ def test_fp64_poles_tracks_the_fp64_oracle_closer(cuda):
     msg = f"FP32 max {e32.max():.3g} mean {e32.mean():.3g}; FP64 poles max {e64.max():.3g} mean {e64.mean():.3g}"
     assert e64.mean() <= e32.mean(), msg
     assert e64.max() <= max(e32.max(), 1e-6), msg
+
+
+def test_blend_batch_sizes_and_autotuner(cuda):
+    """Every staging batch size gives the identical image and gradients within tolerance; the
+    autotuner picks one of the candidates and leaves the state ready for the backward."""
+    g = scenes.make_gaussians(30_000, seed=8)
+    gt = lonlat.GaussianTensors.from_numpy(g)
+    views = _views([(1024, 512), (512, 256)], 8)
+    cams = batch.BatchCameras.from_views(views)
+    dl = [torch.from_numpy(scenes.upstream_grad(v.width, v.height, seed=30 + i)).cuda() for i, v in enumerate(views)]
+    out = {}
+    try:
+        for b in (128, 256, 512):
+            batch.set_blend_batch(b, b)
+            images, per, state = batch.render_batch(gt, cams)
+            grads = batch.BatchGradients.empty(gt.P, gt.M, cuda)
+            state.backward(gt, cams, dl, grads)
+            torch.cuda.synchronize()
+            out[b] = (images, grads)
+        for b in (128, 512):
+            for x, y in zip(out[b][0], out[256][0]):
+                torch.testing.assert_close(x, y, rtol=0, atol=0)
+            for k in ("dL_dmeans3D", "dL_dsh", "dL_dopacity", "dL_dscales", "dL_drotations"):
+                assert _rel(getattr(out[b][1], k), getattr(out[256][1], k)) < GRAD_RTOL, (b, k)
+        batch.set_blend_batch(256, 256)
+        images, per, state = batch.render_batch(gt, cams)
+        res = state.autotune(gt, cams, images, dl)
+        assert res["forward_batch"] in (128, 256, 512) and res["backward_batch"] in (128, 256, 512)
+        assert batch.get_blend_batch() == (res["forward_batch"], res["backward_batch"])
+        assert all(t > 0 for t in res["forward_ms"] + res["backward_ms"])
+        for x, y in zip(images, out[256][0]):
+            torch.testing.assert_close(x, y, rtol=0, atol=0)
+        grads = batch.BatchGradients.empty(gt.P, gt.M, cuda)
+        state.backward(gt, cams, dl, grads)
+        torch.cuda.synchronize()
+        for k in ("dL_dmeans3D", "dL_dsh", "dL_dopacity", "dL_dscales", "dL_drotations"):
+            assert _rel(getattr(grads, k), getattr(out[256][1], k)) < GRAD_RTOL, k
+    finally:
+        batch.set_blend_batch(256, 256)

@@ -238,3 +238,17 @@ def test_adam_validation():
     assert L.omnigs_adam_step(ctypes.byref(prm), ctypes.byref(st), ctypes.byref(act), *([0x10000] * 6),
                               None) == 1
     assert L.omnigs_activate(ctypes.byref(prm), ctypes.byref(act), None) == 1
+
+
+def test_blend_batch_setting():
+    from omnigs_b200 import batch
+    assert batch.get_blend_batch() == (256, 256)
+    with pytest.raises(capi.OmnigsError):
+        batch.set_blend_batch(100, 256)
+    batch.set_blend_batch(128, 512)
+    assert batch.get_blend_batch() == (128, 512)
+    batch.set_blend_batch(256, 256)
+    a, keep = _fake_batch()
+    r = capi.TuneResult()
+    assert capi.lib().omnigs_batch_autotune(ctypes.byref(a), 0x10000, 1 << 40, 0x10000, 1 << 40, 0,
+                                            ctypes.byref(r), None) == 1  # repeats < 1
