@@ -335,13 +335,14 @@ int omnigs_batch_backward(const OmnigsBatchArgs* a, const OmnigsBatchGrads* g, v
   g_last_error.clear();
   BatchPlan plan;
   if (int rc = validate_batch(a, plan)) return rc;
-  if (g == nullptr || g->dL_dmeans3D == nullptr || g->dL_dopacity == nullptr || g->dL_dscales == nullptr ||
+  if (g == nullptr) return fail(OMNIGS_ERR_INVALID_ARGUMENT, "grads is NULL");
+  if (a->P == 0) return OMNIGS_OK;  // no Gaussians, no gradients (the outputs are empty)
+  if (g->dL_dmeans3D == nullptr || g->dL_dopacity == nullptr || g->dL_dscales == nullptr ||
       g->dL_drotations == nullptr || (a->shs != nullptr && a->M > 0 && g->dL_dsh == nullptr))
     return fail(OMNIGS_ERR_INVALID_ARGUMENT, "a required batched gradient output is NULL");
   for (int v = 0; v < a->V; ++v)
     if (a->views[v].dL_dout_color == nullptr)
       return fail(OMNIGS_ERR_INVALID_ARGUMENT, "every view needs dL_dout_color");
-  if (a->P == 0) return OMNIGS_OK;
   const BatchLayout L = batch_layout(a->P, plan);
   if (int rc = check_state(L, state, state_bytes)) return rc;
   int64_t capacity = BinningLayout::capacity_for(binning_bytes);

@@ -203,3 +203,45 @@ def test_blend_batch_sizes_and_autotuner(cuda):
             assert _rel(getattr(grads, k), getattr(out[256][1], k)) < GRAD_RTOL, k
     finally:
         batch.set_blend_batch(256, 256)
+
+
+def test_batch_edge_cases(cuda):
+    """No Gaussians (images are the zeros the reference returns), a view where every Gaussian is
+    culled (camera inside the near-cull sphere of the only Gaussian), and the maximum of 32 views
+    with tiny and ragged sizes, each view matching its single-view render."""
+    bgc = (0.2, 0.4, 0.6)
+    # P = 0
+    empty = lonlat.GaussianTensors(means3D=torch.zeros(0, 3, device=cuda), opacities=torch.zeros(0, 1, device=cuda),
+                                   shs=torch.zeros(0, 16, 3, device=cuda), scales=torch.zeros(0, 3, device=cuda),
+                                   rotations=torch.zeros(0, 4, device=cuda))
+    cams = batch.BatchCameras.from_views([scenes.identity_view(64, 32), scenes.identity_view(48, 16)], background=bgc)
+    st = batch.BatchState(0, cams.sizes, 1024)
+    images = [torch.full((3, h, w), 7.0, device=cuda) for w, h in cams.sizes]
+    st.forward(empty, cams, images)
+    torch.cuda.synchronize()
+    for im in images:
+        assert float(im.abs().max()) == 0.0
+    grads = batch.BatchGradients.empty(0, 16, cuda)
+    st.backward(empty, cams, [torch.zeros(3, h, w, device=cuda) for w, h in cams.sizes], grads)
+    # every Gaussian culled in one view (r^2 <= 0.04 around the camera), visible in the other
+    one = scenes.make_gaussians(1, seed=1)
+    one = scenes.Gaussians(np.array([[0.0, 0.0, 1.0]], np.float32), one.scales, one.rotations, one.opacities, one.shs)
+    g1 = lonlat.GaussianTensors.from_numpy(one)
+    views = [scenes.make_view(64, 32, (0.0, 0.0, 1.05)), scenes.identity_view(64, 32)]
+    images, per, state = batch.render_batch(g1, batch.BatchCameras.from_views(views, background=bgc))
+    assert per[0] == 0 and per[1] > 0
+    torch.testing.assert_close(images[0], torch.tensor(bgc, device=cuda).view(3, 1, 1).expand(3, 32, 64),
+                               rtol=0, atol=0)
+    # 32 views, tiny and ragged sizes, against single-view renders
+    g = scenes.make_gaussians(5_000, seed=12)
+    gt = lonlat.GaussianTensors.from_numpy(g)
+    rng = np.random.Generator(np.random.PCG64(12))
+    sizes = [(int(rng.integers(8, 200)), int(rng.integers(4, 100))) for _ in range(capi.MAX_BATCH_VIEWS)]
+    views = _views(sizes, 12)
+    images, per, state = batch.render_batch(gt, batch.BatchCameras.from_views(views, background=bgc))
+    for v, view in enumerate(views):
+        cu = _plain(gt, view, scenes.upstream_grad(view.width, view.height), bgc)
+        assert per[v] == cu["num_rendered"], v
+        torch.testing.assert_close(images[v], cu["image"], rtol=0, atol=0)
+    with pytest.raises(capi.OmnigsError):
+        batch.BatchState(100, [(64, 32)] * (capi.MAX_BATCH_VIEWS + 1), 1024)
