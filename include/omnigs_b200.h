@@ -212,6 +212,9 @@ typedef struct OmnigsBatchArgs {
   const float* campos;         /* [V,3] device */
   const float* backgrounds;    /* [V,3] device */
   const OmnigsBatchView* views;/* [V] host array */
+  int seam_wrap;               /* 0: the reference's clamped tile rects (default); 1: splats wrap
+                                  across the longitude seam (cyclic tile columns, distances to the
+                                  nearest copy), which removes the seam cut of the reference */
 } OmnigsBatchArgs;
 
 /* Gradient outputs of the batched backward: parameter gradients summed over the views (fully

@@ -6,7 +6,8 @@ single-view path's; the backward returns the parameter gradients summed over the
 accumulates the trainer's densification statistics (per-view viewspace-gradient norms, visible-view
 counts, maximum radii).  SH coefficients may be passed as bfloat16 (``shs.dtype ==
 torch.bfloat16``); ``fp64_poles`` evaluates the 2D covariance of Gaussians beyond 85 degrees of
-latitude in FP64.  Nothing here synchronises the host except ``status()``.
+latitude in FP64; ``seam_wrap`` lets splats wrap across the longitude seam (off: the reference's
+clamped tile rects).  Nothing here synchronises the host except ``status()``.
 """
 from __future__ import annotations
 
@@ -88,7 +89,7 @@ class BatchState:
         self.binning = torch.empty(capi.binning_bytes(capacity), dtype=torch.uint8, device=self.device)
 
     def _args(self, g: GaussianTensors, cams: BatchCameras, images, dL_dimages, D, scale_modifier,
-              fp64_poles):
+              fp64_poles, seam_wrap=False):
         assert cams.sizes == self.sizes and g.P == self.P
         a = capi.BatchArgs()
         a.P, a.D, a.M, a.V = g.P, D, g.M, self.V
@@ -96,6 +97,7 @@ class BatchState:
         assert g.shs is None or g.shs.dtype in (torch.float32, torch.bfloat16)
         a.sh_dtype = capi.SH_BF16 if bf16 else capi.SH_FP32
         a.fp64_poles = 1 if fp64_poles else 0
+        a.seam_wrap = 1 if seam_wrap else 0
         a.means3D = capi.ptr(g.means3D)
         a.shs = capi.ptr(g.shs)
         a.colors_precomp = capi.ptr(g.colors_precomp)
@@ -120,26 +122,27 @@ class BatchState:
         return a, views  # the caller keeps `views` alive for the call
 
     def forward(self, g: GaussianTensors, cams: BatchCameras, images, D: int = 3,
-                scale_modifier: float = 1.0, fp64_poles: bool = False, stream=None):
+                scale_modifier: float = 1.0, fp64_poles: bool = False, stream=None, seam_wrap: bool = False):
         """Asynchronous forward of every view into ``images`` (list of [3,H,W] tensors)."""
-        a, keep = self._args(g, cams, images, None, D, scale_modifier, fp64_poles)
+        a, keep = self._args(g, cams, images, None, D, scale_modifier, fp64_poles, seam_wrap)
         rc = capi.lib().omnigs_batch_forward(ctypes.byref(a), self.state.data_ptr(), self.state.numel(),
                                              self.binning.data_ptr(), self.binning.numel(),
                                              capi.stream_handle(stream))
         capi.check(rc, "omnigs_batch_forward")
 
     def render(self, g: GaussianTensors, cams: BatchCameras, images, D: int = 3,
-               scale_modifier: float = 1.0, fp64_poles: bool = False, stream=None):
+               scale_modifier: float = 1.0, fp64_poles: bool = False, stream=None, seam_wrap: bool = False):
         """Binning + blend again from the current preprocess (after a capacity resize)."""
-        a, keep = self._args(g, cams, images, None, D, scale_modifier, fp64_poles)
+        a, keep = self._args(g, cams, images, None, D, scale_modifier, fp64_poles, seam_wrap)
         rc = capi.lib().omnigs_batch_render(ctypes.byref(a), self.state.data_ptr(), self.state.numel(),
                                             self.binning.data_ptr(), self.binning.numel(),
                                             capi.stream_handle(stream))
         capi.check(rc, "omnigs_batch_render")
 
     def backward(self, g: GaussianTensors, cams: BatchCameras, dL_dimages, grads: BatchGradients,
-                 D: int = 3, scale_modifier: float = 1.0, fp64_poles: bool = False, stream=None):
-        a, keep = self._args(g, cams, None, dL_dimages, D, scale_modifier, fp64_poles)
+                 D: int = 3, scale_modifier: float = 1.0, fp64_poles: bool = False, stream=None,
+                 seam_wrap: bool = False):
+        a, keep = self._args(g, cams, None, dL_dimages, D, scale_modifier, fp64_poles, seam_wrap)
         bg = capi.BatchGrads()
         for f, _ in capi.BatchGrads._fields_:
             setattr(bg, f, capi.ptr(getattr(grads, f)))
@@ -212,18 +215,19 @@ def get_blend_batch() -> tuple[int, int]:
 
 
 def render_batch(g: GaussianTensors, cams: BatchCameras, D: int = 3, scale_modifier: float = 1.0,
-                 fp64_poles: bool = False, capacity: int | None = None, state: BatchState | None = None):
+                 fp64_poles: bool = False, capacity: int | None = None, state: BatchState | None = None,
+                 seam_wrap: bool = False):
     """Forward of every view with exact capacity sizing; returns (images, num_rendered per view,
     state)."""
     dev = g.means3D.device
     if state is None:
         state = BatchState(g.P, cams.sizes, capacity or max(1024, 4 * g.P * cams.V), dev)
     images = [torch.empty(3, h, w, dtype=torch.float32, device=dev) for w, h in cams.sizes]
-    state.forward(g, cams, images, D, scale_modifier, fp64_poles)
+    state.forward(g, cams, images, D, scale_modifier, fp64_poles, seam_wrap=seam_wrap)
     n, per, st = state.status()
     if st & capi.STATUS_CAPACITY:
         state.resize_capacity(n)
-        state.render(g, cams, images, D, scale_modifier, fp64_poles)
+        state.render(g, cams, images, D, scale_modifier, fp64_poles, seam_wrap=seam_wrap)
         n, per, st = state.status()
     if st:
         raise capi.OmnigsError(f"device status bits {st}")

@@ -81,7 +81,7 @@ class BatchArgs(ctypes.Structure):
                 ("means3D", _vp), ("shs", _vp), ("colors_precomp", _vp), ("opacities", _vp),
                 ("scales", _vp), ("scale_modifier", _f), ("rotations", _vp), ("cov3D_precomp", _vp),
                 ("viewmatrices", _vp), ("campos", _vp), ("backgrounds", _vp),
-                ("views", ctypes.POINTER(BatchView))]
+                ("views", ctypes.POINTER(BatchView)), ("seam_wrap", _i)]
 
 
 class BatchGrads(ctypes.Structure):

@@ -113,7 +113,7 @@ __global__ void __launch_bounds__(kBatchBlock) batch_preprocess_kernel(const __g
       const BatchView& bv = p.views[v];
       const SplatResult r = preprocess_splat<kFp64Poles>(
           p_orig, p.viewmatrices + 16 * v, bv.W, bv.H, bv.gx, bv.gy, p.D, p.campos + 3 * v, opacity,
-          p.colors_precomp != nullptr ? p.colors_precomp + 3 * g : nullptr, cov3d, sh);
+          p.colors_precomp != nullptr ? p.colors_precomp + 3 * g : nullptr, p.seam_wrap != 0, cov3d, sh);
       const size_t rec = (size_t)v * p.P + g;
       p.radii[rec] = r.radius;
       p.depth[rec] = r.depth_key;

@@ -76,6 +76,7 @@ int validate_batch(const OmnigsBatchArgs* a, BatchPlan& plan) {
   if (a->sh_dtype != OMNIGS_SH_FP32 && a->sh_dtype != OMNIGS_SH_BF16)
     return fail(OMNIGS_ERR_INVALID_ARGUMENT, "sh_dtype must be OMNIGS_SH_FP32 or OMNIGS_SH_BF16");
   if (a->fp64_poles != 0 && a->fp64_poles != 1) return fail(OMNIGS_ERR_INVALID_ARGUMENT, "fp64_poles must be 0 or 1");
+  if (a->seam_wrap != 0 && a->seam_wrap != 1) return fail(OMNIGS_ERR_INVALID_ARGUMENT, "seam_wrap must be 0 or 1");
   if (a->shs != nullptr && a->M > 16)
     return fail(OMNIGS_ERR_INVALID_ARGUMENT, "batched views support at most 16 SH coefficients per Gaussian");
   if (int rc = validate_common(a->P, a->D, a->M, a->views[0].W, a->views[0].H, a->shs, a->colors_precomp, a->scales,
@@ -96,6 +97,7 @@ BatchParams batch_params(const OmnigsBatchArgs* a, const BatchPlan& plan, void* 
   p.D = a->D;
   p.M = a->shs != nullptr ? a->M : 0;
   p.sh_bf16 = a->sh_dtype == OMNIGS_SH_BF16;
+  p.seam_wrap = a->seam_wrap;
   p.total_tiles = (uint32_t)plan.tiles;
   p.means3D = a->means3D;
   p.scales = a->scales;
@@ -144,6 +146,7 @@ BatchRenderParams render_params(const BatchParams& p, const BatchPlan& plan, voi
   r.n_contrib = at<uint32_t>(state, L.n_contrib);
   r.grad_acc = reinterpret_cast<float*>(p.grad_acc);
   r.total_tiles = (uint32_t)plan.tiles;
+  r.seam_wrap = p.seam_wrap;
   for (int v = 0; v < p.V; ++v) {
     r.views[v] = p.views[v];
     r.tile_order[v] = plan.tile_order[v];
@@ -259,6 +262,7 @@ int omnigs_batch_render(const OmnigsBatchArgs* a, void* state, size_t state_byte
   d.scan_state = at<unsigned long long>(state, L.dup_scan);
   d.capacity = capacity;
   d.hdr = hdr;
+  d.seam_wrap = a->seam_wrap;
   for (int v = 0; v < a->V; ++v) {
     d.gx[v] = bp.views[v].gx;
     d.gy[v] = bp.views[v].gy;

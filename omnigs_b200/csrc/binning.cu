@@ -288,8 +288,8 @@ __global__ void __launch_bounds__(kScanBlock) duplicate_kernel(const __grid_cons
   const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
   const uint32_t items = (uint32_t)p.P * (uint32_t)p.V;
   const uint32_t i = tile * kScanBlock + threadIdx.x;
-  uint32_t count = 0, g = 0, tile_origin = 0;
-  int pitch = 1, width = 1;
+  uint32_t count = 0, g = 0, row_origin = 0;
+  int pitch = 1, width = 1, col0 = 0;
   if (i < items) {
     const uint32_t view = (p.V == 1) ? 0u : i / (uint32_t)p.P;  // the order keeps records in their view
     g = p.order[i];
@@ -298,12 +298,16 @@ __global__ void __launch_bounds__(kScanBlock) duplicate_kernel(const __grid_cons
       const float4 a = p.splat[2 * g];
       const int gx = p.gx[view];
       int2 rmin, rmax;
-      tile_rect(make_float2(a.x, a.y), radius, gx, p.gy[view], rmin, rmax);
+      if (p.seam_wrap)
+        tile_rect_cyclic(make_float2(a.x, a.y), radius, gx, p.gy[view], rmin, rmax);
+      else
+        tile_rect(make_float2(a.x, a.y), radius, gx, p.gy[view], rmin, rmax);
       width = rmax.x - rmin.x;
       count = (uint32_t)width * (uint32_t)(rmax.y - rmin.y);
       if (count == 0) width = 1;
       pitch = gx;
-      tile_origin = p.tile_base[view] + (uint32_t)rmin.y * (uint32_t)gx + (uint32_t)rmin.x;
+      col0 = rmin.x;
+      row_origin = p.tile_base[view] + (uint32_t)rmin.y * (uint32_t)gx;
     }
   }
   // block inclusive scan of the counts
@@ -390,15 +394,18 @@ __global__ void __launch_bounds__(kScanBlock) duplicate_kernel(const __grid_cons
       if (s <= o) pos += step;
     }
     const uint32_t o_start = __shfl_sync(kFullMask, start, pos);
-    const uint32_t o_origin = __shfl_sync(kFullMask, tile_origin, pos);
+    const uint32_t o_origin = __shfl_sync(kFullMask, row_origin, pos);
     const int o_pitch = __shfl_sync(kFullMask, pitch, pos);
     const int o_width = __shfl_sync(kFullMask, width, pos);
+    const int o_col0 = __shfl_sync(kFullMask, col0, pos);
     const uint32_t o_g = __shfl_sync(kFullMask, g, pos);
     if (o < w_end && o < limit) {
       const uint32_t local = o - o_start;
       const uint32_t ry = local / (uint32_t)o_width;
-      const uint32_t rx = local - ry * (uint32_t)o_width;
-      p.tkeys[o] = o_origin + ry * (uint32_t)o_pitch + rx;
+      int tx = o_col0 + (int)(local - ry * (uint32_t)o_width);
+      if (tx < 0) tx += o_pitch;  // seam wrap: columns left of 0 or right of gx - 1
+      if (tx >= o_pitch) tx -= o_pitch;
+      p.tkeys[o] = o_origin + ry * (uint32_t)o_pitch + (uint32_t)tx;
       p.tvals[o] = o_g;
     }
   }

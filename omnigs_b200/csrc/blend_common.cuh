@@ -28,6 +28,7 @@ struct TileJob {
   float* final_T;           // [H*W]
   uint32_t* n_contrib;      // [H*W]
   const float* dL_dpix;     // [3,H,W] (backward)
+  float wrap_w;             // image width when blending across the longitude seam, else 0
 };
 
 // The sorted instance list and the per-record splat data it points into.
@@ -50,8 +51,15 @@ struct BlendPatch {
   int px, py0;       // this thread's column and first row
   float pxf;         // column as float
   float wcx, wcy;    // centre of the warp's patch
+  float wrap_w;      // image width in seam-wrapping mode, else 0
 
-  static __device__ __forceinline__ BlendPatch make(int tile_x, int tile_y) {
+  // x of the splat's copy (shifted by a multiple of the image width) nearest this patch; the
+  // splat's own x unless the seam wraps.
+  __device__ __forceinline__ float center_x(float ax) const {
+    return wrap_w > 0.f ? ax - wrap_w * rintf((ax - wcx) / wrap_w) : ax;
+  }
+
+  static __device__ __forceinline__ BlendPatch make(int tile_x, int tile_y, float wrap_w = 0.f) {
     const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
     const int wx0 = tile_x * 16 + (warp & 1) * 8;
     const int wy0 = tile_y * 16 + (warp >> 1) * 4 * kBlendPx;
@@ -61,6 +69,7 @@ struct BlendPatch {
     b.pxf = (float)b.px;
     b.wcx = (float)wx0 + 3.5f;
     b.wcy = (float)wy0 + 0.5f * (4 * kBlendPx - 1);
+    b.wrap_w = wrap_w;
     return b;
   }
   __device__ __forceinline__ int py(int i) const { return py0 + 4 * i; }
@@ -70,7 +79,7 @@ struct BlendPatch {
   // The splat's alpha-support box (centre a.xy, half extents b.zw) touches the patch.  Written as
   // a negated "misses" test so that NaN extents count as touching (the per-pixel test decides).
   __device__ __forceinline__ bool hit(const float4& a, const float4& b) const {
-    return !(fabsf(a.x - wcx) > b.z + 3.5f || fabsf(a.y - wcy) > b.w + (2.0f * kBlendPx - 0.5f));
+    return !(fabsf(center_x(a.x) - wcx) > b.z + 3.5f || fabsf(a.y - wcy) > b.w + (2.0f * kBlendPx - 0.5f));
   }
 };
 
@@ -150,6 +159,7 @@ __device__ __forceinline__ TileJob batch_tile_job(const BatchRenderParams& p, ui
   job.final_T = p.final_T + bv.pixel_base;
   job.n_contrib = p.n_contrib + bv.pixel_base;
   job.dL_dpix = bv.dL_dpix;
+  job.wrap_w = p.seam_wrap ? (float)bv.W : 0.f;
   return job;
 }
 

@@ -82,6 +82,7 @@ struct DuplicateParams {
   unsigned long long* scan_state;
   int64_t capacity;
   GeomHeader* hdr;
+  int seam_wrap;               // tile columns wrap modulo gx (rects from tile_rect_cyclic)
   int gx[kMaxBatchViews], gy[kMaxBatchViews];
   uint32_t tile_base[kMaxBatchViews];
 };
@@ -150,6 +151,7 @@ struct BatchView {
 struct BatchParams {
   int P, V, D, M;
   int sh_bf16;                  // shs holds bf16 instead of fp32 values
+  int seam_wrap;                // cyclic tile columns and wrapped blend distance
   uint32_t total_tiles;
   const float* means3D;
   const float* scales;
@@ -202,6 +204,7 @@ struct BatchRenderParams {
   uint32_t* n_contrib;          // [total pixels]
   float* grad_acc;              // [V][P][12]
   uint32_t total_tiles;
+  int seam_wrap;                // blend distances to the splat copy nearest each warp patch
   BatchView views[kMaxBatchViews];
   uint8_t tile_order[kMaxBatchViews];  // view indices by ascending tile_base
 };

@@ -113,6 +113,20 @@ __device__ __forceinline__ void tile_rect(float2 p, int max_radius, int gx, int 
   rmax.y = min(gy, max(0, (int)((p.y + max_radius + kTileH - 1) / kTileH)));
 }
 
+// Seam-wrapping variant (the reference's unused getRectCyclic, auxiliary.h:68-83): the tile-column
+// range may start left of column 0 (down to -gx) and end right of gx (up to 2 gx); the caller wraps
+// column indices modulo gx.  Unlike getRectCyclic the left edge is floored, so a splat reaching
+// less than a tile past x = 0 still gets the wrapped column, and the range is capped at one image
+// width so no column is listed twice.  Rows are clamped as in getRect.
+__device__ __forceinline__ void tile_rect_cyclic(float2 p, int max_radius, int gx, int gy, int2& rmin, int2& rmax) {
+  rmin.x = min(gx, max(-gx, (int)floorf((p.x - max_radius) / kTileW)));
+  rmin.y = min(gy, max(0, (int)((p.y - max_radius) / kTileH)));
+  rmax.x = min(2 * gx, max(0, (int)((p.x + max_radius + kTileW - 1) / kTileW)));
+  rmax.y = min(gy, max(0, (int)((p.y + max_radius + kTileH - 1) / kTileH)));
+  if (rmax.x < rmin.x) rmax.x = rmin.x;
+  if (rmax.x - rmin.x > gx) rmax.x = rmin.x + gx;
+}
+
 // 3D covariance from scale and (unnormalised) quaternion (r, x, y, z), forward.cu:194-228.
 __device__ __forceinline__ void cov3d_from_scale_rot(float3 s, float mod, float4 q, float out[6]) {
   Mat3c S = mat3_identity();

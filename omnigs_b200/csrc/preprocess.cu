@@ -40,7 +40,7 @@ __global__ void __launch_bounds__(kScanBlock) preprocess_kernel(PreprocessParams
     auto sh = [shg](int k) { return v3(__ldg(shg + 3 * k), __ldg(shg + 3 * k + 1), __ldg(shg + 3 * k + 2)); };
     const SplatResult r = preprocess_splat</*kFp64Poles=*/false>(
         p_orig, p.viewmatrix, p.W, p.H, p.gx, p.gy, p.D, p.campos, p.opacities[idx],
-        p.colors_precomp != nullptr ? p.colors_precomp + 3 * idx : nullptr, cov3d, sh);
+        p.colors_precomp != nullptr ? p.colors_precomp + 3 * idx : nullptr, /*seam_wrap=*/false, cov3d, sh);
     p.radii[idx] = r.radius;
     if (r.radius > 0) {
       p.splat[2 * idx] = r.s0;

@@ -54,13 +54,14 @@ constexpr float kPoleSinLat = 0.99619469809174553f;  // sin(85 deg)
 // instead of reusing the values above.  The barrier keeps that dataflow (and therefore the same
 // FMA contraction), so radii and tile rects stay bit-identical.  `vm` must point to memory (not
 // registers) for the reload to happen.  sh(k) returns coefficient k as a V3.
+// seam_wrap selects the cyclic tile-column range (tile_rect_cyclic) instead of the clamped one.
 // With kFp64Poles, Gaussians beyond kPoleSinLat get their 2D covariance, conic and radius from an
 // FP64 evaluation of the same formulas (not the reference's arithmetic: a precision mode).
 template <bool kFp64Poles, class Cov3DFn, class ShLoad>
 __device__ __forceinline__ SplatResult preprocess_splat(float3 p_orig, const float* vm, int W, int H,
                                                         int gx, int gy, int D, const float* campos,
                                                         float opacity, const float* color_precomp,
-                                                        Cov3DFn cov3d, ShLoad sh) {
+                                                        bool seam_wrap, Cov3DFn cov3d, ShLoad sh) {
   SplatResult res;
   res.radius = 0;
   res.touched = 0;
@@ -104,7 +105,10 @@ __device__ __forceinline__ SplatResult preprocess_splat(float3 p_orig, const flo
   const float2 point_image = {ndc_to_pixel(scr_x, W), ndc_to_pixel(scr_y, H)};
   const int radius = (int)my_radius;
   int2 rmin, rmax;
-  tile_rect(point_image, radius, gx, gy, rmin, rmax);
+  if (seam_wrap)
+    tile_rect_cyclic(point_image, radius, gx, gy, rmin, rmax);
+  else
+    tile_rect(point_image, radius, gx, gy, rmin, rmax);
   const uint32_t area = (uint32_t)(rmax.x - rmin.x) * (uint32_t)(rmax.y - rmin.y);
   if (area == 0) return res;
   if (color_precomp == nullptr) {

@@ -67,7 +67,7 @@ __device__ __forceinline__ void blend_backward_tile(const TileJob& job, const Bl
   __shared__ float4 s_c[kBatch];
   __shared__ uint32_t s_g[kBatch];
   __shared__ uint32_t s_warp_last[kBlendWarps];
-  const BlendPatch patch = BlendPatch::make(job.tile_x, job.tile_y);
+  const BlendPatch patch = BlendPatch::make(job.tile_x, job.tile_y, job.wrap_w);
   const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
   const uint2 range = job.range;
   const uint32_t n = range.y - range.x;
@@ -128,7 +128,7 @@ __device__ __forceinline__ void blend_backward_tile(const TileJob& job, const Bl
         if (act0 || act1) {
           const float4 a = s_a[jj];
           const float4 b = s_b[jj];
-          const float dx = a.x - patch.pxf;
+          const float dx = patch.center_x(a.x) - patch.pxf;
           const float2 dy = sub2(f2(a.y), pyf);
           const float2 power = splat_power2(a, b, dx, dy);
           const float2 G = make_float2(expf(power.x), expf(power.y));
@@ -211,6 +211,7 @@ __global__ void __launch_bounds__(kBlendThreads) render_backward_kernel(RenderPa
   job.final_T = p.final_T;
   job.n_contrib = p.n_contrib;
   job.dL_dpix = p.dL_dpix;
+  job.wrap_w = 0.f;
   blend_backward_tile<kBatch>(job, BlendSource{p.point_list, p.splat, p.color, (uint32_t)p.P, p.capacity}, p.grad_acc);
 }
 

@@ -26,7 +26,7 @@ __device__ __forceinline__ void blend_forward_tile(const TileJob& job, const Ble
   __shared__ float4 s_a[kBatch];  // x, y, conic a, conic b
   __shared__ float4 s_b[kBatch];  // conic c, opacity, cull half-width, cull half-height
   __shared__ float4 s_c[kBatch];  // r, g, b, clamp bits
-  const BlendPatch patch = BlendPatch::make(job.tile_x, job.tile_y);
+  const BlendPatch patch = BlendPatch::make(job.tile_x, job.tile_y, job.wrap_w);
   const int lane = threadIdx.x & 31;
   const uint2 range = job.range;
   const int n = (int)(range.y - range.x);
@@ -54,7 +54,7 @@ __device__ __forceinline__ void blend_forward_tile(const TileJob& job, const Ble
         if (!(done0 && done1)) {
           const float4 a = s_a[jj];
           const float4 b = s_b[jj];
-          const float dx = a.x - patch.pxf;
+          const float dx = patch.center_x(a.x) - patch.pxf;
           const float2 dy = sub2(f2(a.y), pyf);
           const float2 power = splat_power2(a, b, dx, dy);
           const float2 alpha = make_float2(fminf(0.99f, b.y * expf(power.x)), fminf(0.99f, b.y * expf(power.y)));
@@ -120,6 +120,7 @@ __global__ void __launch_bounds__(kBlendThreads) render_forward_kernel(RenderPar
   job.final_T = p.final_T;
   job.n_contrib = p.n_contrib;
   job.dL_dpix = nullptr;
+  job.wrap_w = 0.f;
   blend_forward_tile<kBatch>(job, BlendSource{p.point_list, p.splat, p.color, (uint32_t)p.P, p.capacity});
 }
 

@@ -245,3 +245,46 @@ def test_batch_edge_cases(cuda):
         torch.testing.assert_close(images[v], cu["image"], rtol=0, atol=0)
     with pytest.raises(capi.OmnigsError):
         batch.BatchState(100, [(64, 32)] * (capi.MAX_BATCH_VIEWS + 1), 1024)
+
+
+def test_seam_wrap_turns_yaw_into_a_roll(cuda):
+    """With seam wrapping, turning the camera by k pixels' worth of yaw rolls the equirect image by
+    k pixels (up to FP32 rounding of the projection); with the reference's clamped tile rects the
+    image is cut at the seam, so the columns at both seams differ."""
+    W, H, k = 512, 256, 100
+    g = scenes.make_gaussians(20_000, seed=13)
+    gt = lonlat.GaussianTensors.from_numpy(g)
+    yaw = 2 * np.pi * k / W
+    views = [scenes.identity_view(W, H), scenes.make_view(W, H, (0.0, 0.0, 0.0), scenes.rotation_yaw_pitch(yaw, 0.0))]
+    cams = batch.BatchCameras.from_views(views)
+    seam = torch.zeros(W, dtype=torch.bool, device=cuda)
+    for c in (W - k, 0):  # image 0's seam after the roll, image 1's own seam
+        for d in range(-6, 6):
+            seam[(c + d) % W] = True
+    err = {}
+    for wrap in (False, True):
+        imgs, _, state = batch.render_batch(gt, cams, seam_wrap=wrap)
+        diff = (torch.roll(imgs[0], shifts=-k, dims=2) - imgs[1]).abs()
+        err[wrap] = (float(diff[:, :, seam].mean()), float(diff[:, :, ~seam].mean()))
+        dl = [torch.from_numpy(scenes.upstream_grad(W, H, seed=40 + i)).cuda() for i in range(2)]
+        grads = batch.BatchGradients.empty(gt.P, gt.M, cuda)
+        state.backward(gt, cams, dl, grads, seam_wrap=wrap)
+        torch.cuda.synchronize()
+        assert all(bool(torch.isfinite(getattr(grads, n)).all()) for n in ("dL_dmeans3D", "dL_dsh", "dL_dscales"))
+    assert err[False][0] > 20 * err[False][1], err       # the clamped rects cut the image at the seam
+    assert err[True][0] < 3 * err[True][1] + 1e-5, err    # wrapped: the seam is like any other column
+    assert err[True][0] < 0.05 * err[False][0], err
+
+
+def test_seam_wrap_changes_nothing_away_from_the_seam(cuda):
+    """Gaussians whose tile rects stay inside the image get identical instances and images."""
+    g = scenes.make_gaussians(5_000, seed=14)
+    m = g.means3D.copy()
+    m[:, 2] = np.abs(m[:, 2]) + 1.5        # in front of the camera: longitude within (-90, 90) deg
+    g = scenes.Gaussians(m, g.scales, g.rotations, g.opacities, g.shs)
+    gt = lonlat.GaussianTensors.from_numpy(g)
+    cams = batch.BatchCameras.from_views([scenes.identity_view(512, 256)])
+    a, pa, _ = batch.render_batch(gt, cams, seam_wrap=False)
+    b, pb, _ = batch.render_batch(gt, cams, seam_wrap=True)
+    assert pa == pb
+    torch.testing.assert_close(a[0], b[0], rtol=0, atol=0)
