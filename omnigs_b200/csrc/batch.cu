@@ -179,7 +179,9 @@ __global__ void __launch_bounds__(kBatchBlock) batch_preprocess_backward_kernel(
     const float4 g2 = p.grad_acc[3 * rec + 2];
     const float* vm = p.viewmatrices + 16 * v;
     const int W = p.views[v].W, H = p.views[v].H;
-    const float3 dconic = {g0.z, g0.w, g1.x};
+    // the blend sums the mean and conic terms without their constant factors (render_bwd.cu)
+    const float3 dconic = {-0.5f * g0.z, -0.5f * g0.w, -0.5f * g1.x};
+    const float dm2x = -0.5f * (float)W * g0.x, dm2y = -0.5f * (float)H * g0.y;
     float dcov_v[6];
     LonlatJacobian jac;
     V3 dm;
@@ -194,7 +196,7 @@ __global__ void __launch_bounds__(kBatchBlock) batch_preprocess_backward_kernel(
       dm = cov2d_lonlat_backward<float>(mean, cov3D, vm, W, H, dconic, dcov_v, jac);
 #pragma unroll
     for (int k = 0; k < 6; ++k) dcov[k] += dcov_v[k];
-    dm = dm + mean2d_backward(jac, g0.x, g0.y, W, H, vm);
+    dm = dm + mean2d_backward(jac, dm2x, dm2y, W, H, vm);
     const V3 dcol = v3(g1.z, g1.w, g2.x);
     if (with_sh) {
       const float* cp = p.campos + 3 * v;
@@ -204,7 +206,7 @@ __global__ void __launch_bounds__(kBatchBlock) batch_preprocess_backward_kernel(
     dmean = dmean + dm;
     dcolor = dcolor + dcol;
     dopacity += g1.y;
-    stat_norm += sqrtf(g0.x * g0.x + g0.y * g0.y);
+    stat_norm += sqrtf(dm2x * dm2x + dm2y * dm2y);
     stat_views += 1.f;
     max_radius = max(max_radius, radius);
   }

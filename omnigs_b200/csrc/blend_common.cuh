@@ -54,9 +54,11 @@ struct BlendPatch {
   float wrap_w;      // image width in seam-wrapping mode, else 0
 
   // x of the splat's copy (shifted by a multiple of the image width) nearest this patch; the
-  // splat's own x unless the seam wraps.
+  // splat's own x unless the seam wraps (kWrap, a template flag so that the non-wrapping kernels
+  // carry no trace of it).
+  template <bool kWrap>
   __device__ __forceinline__ float center_x(float ax) const {
-    return wrap_w > 0.f ? ax - wrap_w * rintf((ax - wcx) / wrap_w) : ax;
+    return kWrap ? ax - wrap_w * rintf((ax - wcx) / wrap_w) : ax;
   }
 
   static __device__ __forceinline__ BlendPatch make(int tile_x, int tile_y, float wrap_w = 0.f) {
@@ -78,8 +80,9 @@ struct BlendPatch {
   __device__ __forceinline__ int64_t pixel(int i, int W) const { return (int64_t)py(i) * W + px; }
   // The splat's alpha-support box (centre a.xy, half extents b.zw) touches the patch.  Written as
   // a negated "misses" test so that NaN extents count as touching (the per-pixel test decides).
+  template <bool kWrap>
   __device__ __forceinline__ bool hit(const float4& a, const float4& b) const {
-    return !(fabsf(center_x(a.x) - wcx) > b.z + 3.5f || fabsf(a.y - wcy) > b.w + (2.0f * kBlendPx - 0.5f));
+    return !(fabsf(center_x<kWrap>(a.x) - wcx) > b.z + 3.5f || fabsf(a.y - wcy) > b.w + (2.0f * kBlendPx - 0.5f));
   }
 };
 

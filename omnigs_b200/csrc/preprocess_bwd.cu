@@ -47,17 +47,18 @@ __global__ void __launch_bounds__(256) preprocess_backward_kernel(PreprocessBack
   p.grad_acc[3 * idx] = z4;
   p.grad_acc[3 * idx + 1] = z4;
   p.grad_acc[3 * idx + 2] = z4;
-  const float dmean2D_x = g0.x, dmean2D_y = g0.y;
-  const float3 dL_dconic = {g0.z, g0.w, g1.x};
+  // the blend sums the mean and conic terms without their constant factors (render_bwd.cu)
+  const float dmean2D_x = -0.5f * (float)p.W * g0.x, dmean2D_y = -0.5f * (float)p.H * g0.y;
+  const float3 dL_dconic = {-0.5f * g0.z, -0.5f * g0.w, -0.5f * g1.x};
   const float dL_dcolor[3] = {g1.z, g1.w, g2.x};
   p.dL_dmeans2D[3 * idx] = dmean2D_x;
   p.dL_dmeans2D[3 * idx + 1] = dmean2D_y;
   p.dL_dmeans2D[3 * idx + 2] = 0.f;
   if (p.dL_dconic) {
-    p.dL_dconic[4 * idx] = g0.z;
-    p.dL_dconic[4 * idx + 1] = g0.w;
+    p.dL_dconic[4 * idx] = dL_dconic.x;
+    p.dL_dconic[4 * idx + 1] = dL_dconic.y;
     p.dL_dconic[4 * idx + 2] = 0.f;
-    p.dL_dconic[4 * idx + 3] = g1.x;
+    p.dL_dconic[4 * idx + 3] = dL_dconic.z;
   }
   p.dL_dopacity[idx] = g1.y;
   p.dL_dcolors[3 * idx] = dL_dcolor[0];

@@ -9,7 +9,9 @@
 // 1 - alpha serves both of the reference's divisions by it (relative error ~1e-7 per step, far
 // inside the gradients' 1e-3 tolerance).  The per-(pixel, splat) gradients (2 screen-space mean,
 // 3 conic, 1 opacity, 3 colour) are not pushed with 9 global atomics per pixel as in the
-// reference: a thread first sums them over its two pixels, the warp that owns the 8 x 8 patch
+// reference (and the mean and conic terms are summed without their constant factors -W/2, -H/2,
+// -1/2, which the backward preprocess applies per Gaussian): a thread first sums them over its two
+// pixels, the warp that owns the 8 x 8 patch
 // reduces them with a reduce-scatter of 8 values (9 shuffles) plus a butterfly for the ninth, and
 // 8 lanes add one accumulator record per splat; when a single lane contributes it adds its 9
 // values directly.  Warps skip splats whose alpha-support box misses their patch or that lie
@@ -59,7 +61,7 @@ __device__ __forceinline__ float rcp_approx(float x) {
   return r;
 }
 
-template <int kBatch>
+template <int kBatch, bool kWrap>
 __device__ __forceinline__ void blend_backward_tile(const TileJob& job, const BlendSource& src, float* grad_acc) {
   static_assert(kBlendPx == 2, "the backward blend packs a thread's two pixels into f32x2 lanes");
   __shared__ float4 s_a[kBatch];
@@ -98,8 +100,6 @@ __device__ __forceinline__ void blend_backward_tile(const TileJob& job, const Bl
   // colour of everything behind the current splat, accumulated back to front
   float2 acc0 = make_float2(0.f, 0.f), acc1 = acc0, acc2 = acc0;
   const float2 pyf = make_float2(patch.pyf(0), patch.pyf(1));
-  const float ddelx_dx = 0.5 * job.W;
-  const float ddely_dy = 0.5 * job.H;
 
   const uint32_t warp_last = __reduce_max_sync(kFullMask, max(lc[0], lc[1]));
   if (lane == 0) s_warp_last[warp] = warp_last;
@@ -116,7 +116,7 @@ __device__ __forceinline__ void blend_backward_tile(const TileJob& job, const Bl
     for (int k = 0; k * 32 < cnt; ++k) {
       const int j = k * 32 + lane;
       bool hit = false;
-      if (j < cnt && (uint32_t)(hi - 1 - j) < warp_last) hit = patch.hit(s_a[j], s_b[j]);
+      if (j < cnt && (uint32_t)(hi - 1 - j) < warp_last) hit = patch.template hit<kWrap>(s_a[j], s_b[j]);
       unsigned m = __ballot_sync(kFullMask, hit);
       while (m) {
         const int jj = k * 32 + __ffs(m) - 1;
@@ -128,7 +128,7 @@ __device__ __forceinline__ void blend_backward_tile(const TileJob& job, const Bl
         if (act0 || act1) {
           const float4 a = s_a[jj];
           const float4 b = s_b[jj];
-          const float dx = patch.center_x(a.x) - patch.pxf;
+          const float dx = patch.template center_x<kWrap>(a.x) - patch.pxf;
           const float2 dy = sub2(f2(a.y), pyf);
           const float2 power = splat_power2(a, b, dx, dy);
           const float2 G = make_float2(expf(power.x), expf(power.y));
@@ -146,27 +146,28 @@ __device__ __forceinline__ void blend_backward_tile(const TileJob& job, const Bl
             T = mul2(T, inv);  // transmittance in front of this splat
             const float2 dcd = mul2(ae, T);
             const float4 cv = s_c[jj];
-            float2 dLda = mul2(sub2(f2(cv.x), acc0), dp0);
-            dLda = fma2(sub2(f2(cv.y), acc1), dp1, dLda);
-            dLda = fma2(sub2(f2(cv.z), acc2), dp2, dLda);
-            acc0 = fma2(ae, f2(cv.x), mul2(onem, acc0));
-            acc1 = fma2(ae, f2(cv.y), mul2(onem, acc1));
-            acc2 = fma2(ae, f2(cv.z), mul2(onem, acc2));
+            // colour of this splat minus the colour behind it, per channel
+            const float2 e0 = sub2(f2(cv.x), acc0), e1 = sub2(f2(cv.y), acc1), e2 = sub2(f2(cv.z), acc2);
+            float2 dLda = mul2(e0, dp0);
+            dLda = fma2(e1, dp1, dLda);
+            dLda = fma2(e2, dp2, dLda);
+            acc0 = fma2(ae, e0, acc0);  // alpha c + (1 - alpha) acc
+            acc1 = fma2(ae, e1, acc1);
+            acc2 = fma2(ae, e2, acc2);
             dLda = mul2(dLda, T);
             dLda = fma2(mul2(neg_T_final, inv), bgdot, dLda);
-            const float2 dLdG = mul2(f2(b.y), dLda);
-            const float2 gdx = mul2(Ge, f2(dx));
-            const float2 gdy = mul2(Ge, dy);
-            // dG/d(delta x) = -gdx a - gdy b, dG/d(delta y) = -gdy c - gdx b (conic a, b, c)
-            const float2 dGdx = fma2(gdx, f2(-a.z), mul2(gdy, f2(-a.w)));
-            const float2 dGdy = fma2(gdy, f2(-b.x), mul2(gdx, f2(-a.w)));
-            const float2 hd = mul2(f2(-0.5f), dLdG);
-            const float2 w0 = mul2(mul2(dLdG, dGdx), f2(ddelx_dx));
-            const float2 w1 = mul2(mul2(dLdG, dGdy), f2(ddely_dy));
-            const float2 w2 = mul2(mul2(gdx, f2(dx)), hd);
-            const float2 w3 = mul2(mul2(gdx, dy), hd);
-            const float2 w4 = mul2(mul2(gdy, dy), hd);
+            // With q = G dL/dG = o G dL/dalpha and the conic (a, b, c):
+            //   dL/d(delta x) = -q (a dx + b dy), dL/d(delta y) = -q (c dy + b dx),
+            //   dL/d(conic) = -q (dx^2, dx dy, dy^2) / 2.
+            // The per-pixel sums keep only q (a dx + b dy), ...; the constant factors -W/2, -H/2 and
+            // -1/2 are applied once per Gaussian by the backward preprocess.
             const float2 w5 = mul2(Ge, dLda);
+            const float2 q = mul2(f2(b.y), w5);
+            const float2 w0 = mul2(q, fma2(f2(a.w), dy, f2(__fmul_rn(a.z, dx))));
+            const float2 w1 = mul2(q, fma2(f2(b.x), dy, f2(__fmul_rn(a.w, dx))));
+            const float2 w2 = mul2(q, f2(dx * dx));
+            const float2 w3 = mul2(q, mul2(f2(dx), dy));
+            const float2 w4 = mul2(q, mul2(dy, dy));
             const float2 w6 = mul2(dcd, dp0);
             const float2 w7 = mul2(dcd, dp1);
             const float2 w8 = mul2(dcd, dp2);
@@ -212,15 +213,24 @@ __global__ void __launch_bounds__(kBlendThreads) render_backward_kernel(RenderPa
   job.n_contrib = p.n_contrib;
   job.dL_dpix = p.dL_dpix;
   job.wrap_w = 0.f;
-  blend_backward_tile<kBatch>(job, BlendSource{p.point_list, p.splat, p.color, (uint32_t)p.P, p.capacity}, p.grad_acc);
+  blend_backward_tile<kBatch, false>(job, BlendSource{p.point_list, p.splat, p.color, (uint32_t)p.P, p.capacity}, p.grad_acc);
 }
 
 // All views of a batch in one launch: block b back-propagates global tile b.
-template <int kBatch>
+template <int kBatch, bool kWrap>
 __global__ void __launch_bounds__(kBlendThreads) batch_render_backward_kernel(const __grid_constant__ BatchRenderParams p) {
   const TileJob job = batch_tile_job(p, blockIdx.x);
-  blend_backward_tile<kBatch>(job, BlendSource{p.point_list, p.splat, p.color, (uint32_t)p.P * (uint32_t)p.V, p.capacity},
+  blend_backward_tile<kBatch, kWrap>(job, BlendSource{p.point_list, p.splat, p.color, (uint32_t)p.P * (uint32_t)p.V, p.capacity},
                       p.grad_acc);
+}
+
+template <bool kWrap>
+void launch_batch_blend(const BatchRenderParams& p, cudaStream_t s) {
+  switch (blend_batch_size(true)) {
+    case 128: batch_render_backward_kernel<128, kWrap><<<p.total_tiles, kBlendThreads, 0, s>>>(p); break;
+    case 512: batch_render_backward_kernel<512, kWrap><<<p.total_tiles, kBlendThreads, 0, s>>>(p); break;
+    default: batch_render_backward_kernel<256, kWrap><<<p.total_tiles, kBlendThreads, 0, s>>>(p); break;
+  }
 }
 
 }  // namespace
@@ -237,11 +247,10 @@ void launch_render_backward(const RenderParams& p, cudaStream_t s) {
 
 void launch_batch_render_backward(const BatchRenderParams& p, cudaStream_t s) {
   if (p.total_tiles == 0) return;
-  switch (blend_batch_size(true)) {
-    case 128: batch_render_backward_kernel<128><<<p.total_tiles, kBlendThreads, 0, s>>>(p); break;
-    case 512: batch_render_backward_kernel<512><<<p.total_tiles, kBlendThreads, 0, s>>>(p); break;
-    default: batch_render_backward_kernel<256><<<p.total_tiles, kBlendThreads, 0, s>>>(p); break;
-  }
+  if (p.seam_wrap)
+    launch_batch_blend<true>(p, s);
+  else
+    launch_batch_blend<false>(p, s);
 }
 
 }  // namespace omnigs

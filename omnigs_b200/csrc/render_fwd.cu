@@ -20,7 +20,7 @@
 namespace omnigs {
 namespace {
 
-template <int kBatch>
+template <int kBatch, bool kWrap>
 __device__ __forceinline__ void blend_forward_tile(const TileJob& job, const BlendSource& src) {
   static_assert(kBlendPx == 2, "the forward blend packs a thread's two pixels into f32x2 lanes");
   __shared__ float4 s_a[kBatch];  // x, y, conic a, conic b
@@ -46,7 +46,7 @@ __device__ __forceinline__ void blend_forward_tile(const TileJob& job, const Ble
     for (int k = 0; k * 32 < cnt && !warp_done; ++k) {
       const int j = k * 32 + lane;
       bool hit = false;
-      if (j < cnt) hit = patch.hit(s_a[j], s_b[j]);
+      if (j < cnt) hit = patch.template hit<kWrap>(s_a[j], s_b[j]);
       unsigned m = __ballot_sync(kFullMask, hit);
       while (m) {
         const int jj = k * 32 + __ffs(m) - 1;
@@ -54,7 +54,7 @@ __device__ __forceinline__ void blend_forward_tile(const TileJob& job, const Ble
         if (!(done0 && done1)) {
           const float4 a = s_a[jj];
           const float4 b = s_b[jj];
-          const float dx = patch.center_x(a.x) - patch.pxf;
+          const float dx = patch.template center_x<kWrap>(a.x) - patch.pxf;
           const float2 dy = sub2(f2(a.y), pyf);
           const float2 power = splat_power2(a, b, dx, dy);
           const float2 alpha = make_float2(fminf(0.99f, b.y * expf(power.x)), fminf(0.99f, b.y * expf(power.y)));
@@ -121,14 +121,23 @@ __global__ void __launch_bounds__(kBlendThreads) render_forward_kernel(RenderPar
   job.n_contrib = p.n_contrib;
   job.dL_dpix = nullptr;
   job.wrap_w = 0.f;
-  blend_forward_tile<kBatch>(job, BlendSource{p.point_list, p.splat, p.color, (uint32_t)p.P, p.capacity});
+  blend_forward_tile<kBatch, false>(job, BlendSource{p.point_list, p.splat, p.color, (uint32_t)p.P, p.capacity});
 }
 
 // All views of a batch in one launch: block b blends global tile b.
-template <int kBatch>
+template <int kBatch, bool kWrap>
 __global__ void __launch_bounds__(kBlendThreads) batch_render_forward_kernel(const __grid_constant__ BatchRenderParams p) {
   const TileJob job = batch_tile_job(p, blockIdx.x);
-  blend_forward_tile<kBatch>(job, BlendSource{p.point_list, p.splat, p.color, (uint32_t)p.P * (uint32_t)p.V, p.capacity});
+  blend_forward_tile<kBatch, kWrap>(job, BlendSource{p.point_list, p.splat, p.color, (uint32_t)p.P * (uint32_t)p.V, p.capacity});
+}
+
+template <bool kWrap>
+void launch_batch_blend(const BatchRenderParams& p, cudaStream_t s) {
+  switch (blend_batch_size(false)) {
+    case 128: batch_render_forward_kernel<128, kWrap><<<p.total_tiles, kBlendThreads, 0, s>>>(p); break;
+    case 512: batch_render_forward_kernel<512, kWrap><<<p.total_tiles, kBlendThreads, 0, s>>>(p); break;
+    default: batch_render_forward_kernel<256, kWrap><<<p.total_tiles, kBlendThreads, 0, s>>>(p); break;
+  }
 }
 
 }  // namespace
@@ -145,11 +154,10 @@ void launch_render_forward(const RenderParams& p, cudaStream_t s) {
 
 void launch_batch_render_forward(const BatchRenderParams& p, cudaStream_t s) {
   if (p.total_tiles == 0) return;
-  switch (blend_batch_size(false)) {
-    case 128: batch_render_forward_kernel<128><<<p.total_tiles, kBlendThreads, 0, s>>>(p); break;
-    case 512: batch_render_forward_kernel<512><<<p.total_tiles, kBlendThreads, 0, s>>>(p); break;
-    default: batch_render_forward_kernel<256><<<p.total_tiles, kBlendThreads, 0, s>>>(p); break;
-  }
+  if (p.seam_wrap)
+    launch_batch_blend<true>(p, s);
+  else
+    launch_batch_blend<false>(p, s);
 }
 
 }  // namespace omnigs
