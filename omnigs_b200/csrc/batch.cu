@@ -17,58 +17,15 @@
 //
 // Precision mode (template flags): SH read as BF16 (colour and gradients still accumulate in FP32)
 // and FP64 for the 2D covariance, its inverse and its backward beyond 85 degrees of latitude.
-#include <cuda_bf16.h>
-
 #include "kernels.h"
 #include "preprocess_bwd_common.cuh"
 #include "preprocess_common.cuh"
+#include "sh_io.cuh"
 
 namespace omnigs {
 namespace {
 
 constexpr int kBatchBlock = 128;
-constexpr int kMaxShCoeffs = 16;
-
-// Coefficients [0, 16) of Gaussian g (zeros beyond M) into out[48], RGB inner.
-template <bool kShBf16>
-__device__ __forceinline__ void load_sh(const void* shs, int g, int M, float out[3 * kMaxShCoeffs]) {
-  const size_t off = (size_t)g * M * 3;
-  if (kShBf16) {
-    const __nv_bfloat16* base = static_cast<const __nv_bfloat16*>(shs) + off;
-    if (M == kMaxShCoeffs && (reinterpret_cast<uintptr_t>(base) & 15) == 0) {
-      const uint4* v = reinterpret_cast<const uint4*>(base);
-#pragma unroll
-      for (int i = 0; i < 6; ++i) {
-        const uint4 u = __ldg(v + i);
-        const uint32_t w[4] = {u.x, u.y, u.z, u.w};
-#pragma unroll
-        for (int k = 0; k < 4; ++k) {
-          out[8 * i + 2 * k] = __uint_as_float(w[k] << 16);
-          out[8 * i + 2 * k + 1] = __uint_as_float(w[k] & 0xffff0000u);
-        }
-      }
-    } else {
-#pragma unroll
-      for (int i = 0; i < 3 * kMaxShCoeffs; ++i) out[i] = (i < 3 * M) ? __bfloat162float(base[i]) : 0.f;
-    }
-  } else {
-    const float* base = static_cast<const float*>(shs) + off;
-    if (M == kMaxShCoeffs && (reinterpret_cast<uintptr_t>(base) & 15) == 0) {
-      const float4* v = reinterpret_cast<const float4*>(base);
-#pragma unroll
-      for (int i = 0; i < 12; ++i) {
-        const float4 f = __ldg(v + i);
-        out[4 * i] = f.x;
-        out[4 * i + 1] = f.y;
-        out[4 * i + 2] = f.z;
-        out[4 * i + 3] = f.w;
-      }
-    } else {
-#pragma unroll
-      for (int i = 0; i < 3 * kMaxShCoeffs; ++i) out[i] = (i < 3 * M) ? __ldg(base + i) : 0.f;
-    }
-  }
-}
 
 // The Gaussian's 3D covariance: precomputed, or from scale and rotation (forward.cu:194-228).
 __device__ __forceinline__ void gaussian_cov3d(const BatchParams& p, int g, float out[6]) {
@@ -215,26 +172,8 @@ __global__ void __launch_bounds__(kBatchBlock) batch_preprocess_backward_kernel(
   out.dL_dmeans3D[3 * g + 1] = dmean.y;
   out.dL_dmeans3D[3 * g + 2] = dmean.z;
   out.dL_dopacity[g] = dopacity;
-  if (out.dL_dsh != nullptr && p.M > 0) {
-    const int ncoef = (p.D + 1) * (p.D + 1);
-    float* d = out.dL_dsh + (size_t)g * p.M * 3;
-    if (p.M == kMaxShCoeffs && (reinterpret_cast<uintptr_t>(d) & 15) == 0) {
-#pragma unroll
-      for (int i = 0; i < 12; ++i) {
-        float4 f;
-        f.x = (4 * i < 3 * ncoef && with_sh) ? dsh[4 * i] : 0.f;
-        f.y = (4 * i + 1 < 3 * ncoef && with_sh) ? dsh[4 * i + 1] : 0.f;
-        f.z = (4 * i + 2 < 3 * ncoef && with_sh) ? dsh[4 * i + 2] : 0.f;
-        f.w = (4 * i + 3 < 3 * ncoef && with_sh) ? dsh[4 * i + 3] : 0.f;
-        reinterpret_cast<float4*>(d)[i] = f;
-      }
-    } else {
-#pragma unroll
-      for (int i = 0; i < 3 * kMaxShCoeffs; ++i)
-        if (i < 3 * p.M) d[i] = (i < 3 * ncoef && with_sh) ? dsh[i] : 0.f;
-      for (int i = 3 * kMaxShCoeffs; i < 3 * p.M; ++i) d[i] = 0.f;
-    }
-  }
+  if (out.dL_dsh != nullptr && p.M > 0)
+    store_sh_grad(out.dL_dsh + (size_t)g * p.M * 3, p.M, with_sh ? (p.D + 1) * (p.D + 1) : 0, dsh);
   if (p.scales != nullptr && p.cov3D_precomp == nullptr) {
     const float3 s = {p.scales[3 * g], p.scales[3 * g + 1], p.scales[3 * g + 2]};
     const float4 q = {p.rotations[4 * g], p.rotations[4 * g + 1], p.rotations[4 * g + 2], p.rotations[4 * g + 3]};

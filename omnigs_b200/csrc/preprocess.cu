@@ -13,6 +13,7 @@
 // for a whole warp without changing any per-pixel decision.
 #include "kernels.h"
 #include "preprocess_common.cuh"
+#include "sh_io.cuh"
 
 namespace omnigs {
 namespace {
@@ -36,8 +37,9 @@ __global__ void __launch_bounds__(kScanBlock) preprocess_kernel(PreprocessParams
         cov3d_from_scale_rot(s, p.scale_modifier, q, out);
       }
     };
-    const float* shg = p.shs != nullptr ? p.shs + (size_t)idx * p.M * 3 : nullptr;
-    auto sh = [shg](int k) { return v3(__ldg(shg + 3 * k), __ldg(shg + 3 * k + 1), __ldg(shg + 3 * k + 2)); };
+    float shv[3 * kMaxShCoeffs];
+    if (p.shs != nullptr) load_sh<false>(p.shs, idx, p.M, shv);
+    auto sh = [&](int k) { return v3(shv[3 * k], shv[3 * k + 1], shv[3 * k + 2]); };
     const SplatResult r = preprocess_splat</*kFp64Poles=*/false>(
         p_orig, p.viewmatrix, p.W, p.H, p.gx, p.gy, p.D, p.campos, p.opacities[idx],
         p.colors_precomp != nullptr ? p.colors_precomp + 3 * idx : nullptr, /*seam_wrap=*/false, cov3d, sh);

@@ -12,6 +12,7 @@
 #include "kernels.h"
 #include "lonlat_math.cuh"
 #include "preprocess_bwd_common.cuh"
+#include "sh_io.cuh"
 
 namespace omnigs {
 namespace {
@@ -87,19 +88,20 @@ __global__ void __launch_bounds__(256) preprocess_backward_kernel(PreprocessBack
 
   // ---- computeColorFromSH backward (backward.cu:30-151) ----
   if (p.shs != nullptr && dsh != nullptr) {
-    const float* shg = p.shs + (size_t)idx * M * 3;
-    auto sh = [shg](int k) { return v3(__ldg(shg + 3 * k), __ldg(shg + 3 * k + 1), __ldg(shg + 3 * k + 2)); };
-    auto put = [dsh](int k, V3 g) {
-      dsh[3 * k] = g.x;
-      dsh[3 * k + 1] = g.y;
-      dsh[3 * k + 2] = g.z;
+    float shv[3 * kMaxShCoeffs], dshv[3 * kMaxShCoeffs];
+    load_sh<false>(p.shs, idx, M, shv);
+    auto sh = [&](int k) { return v3(shv[3 * k], shv[3 * k + 1], shv[3 * k + 2]); };
+    auto put = [&](int k, V3 g) {
+      dshv[3 * k] = g.x;
+      dshv[3 * k + 1] = g.y;
+      dshv[3 * k + 2] = g.z;
     };
     const int deg = p.D;
     const uint32_t clamp_bits = __float_as_uint(p.color[idx].w);
     dL_dmeans = dL_dmeans + sh_backward(deg, v3(mean.x, mean.y, mean.z),
                                         v3(p.campos[0], p.campos[1], p.campos[2]), sh, clamp_bits,
                                         v3(dL_dcolor[0], dL_dcolor[1], dL_dcolor[2]), put);
-    for (int k = (deg + 1) * (deg + 1); k < M; ++k) put(k, v3(0.f, 0.f, 0.f));
+    store_sh_grad(dsh, M, (deg + 1) * (deg + 1), dshv);
   } else if (dsh != nullptr) {
     for (int k = 0; k < 3 * M; ++k) dsh[k] = 0.f;
   }
