@@ -305,10 +305,9 @@ __global__ void __launch_bounds__(256) adam_gaussian_kernel(const __grid_constan
   const int64_t rest_n = (int64_t)P * (M - 1) * 3;
   if (threadIdx.x < 6) s_sc[threadIdx.x] = adam_scalars(*p.hyper, threadIdx.x);
   __syncthreads();
-  // grid-stride over [0, P) (per-Gaussian groups) and [P, P + rest_n) (f_rest elements)
-  for (int64_t i = (int64_t)blockIdx.x * blockDim.x + threadIdx.x; i < P + rest_n;
-       i += (int64_t)gridDim.x * blockDim.x) {
-  if (i < P) {
+  const int64_t stride = (int64_t)gridDim.x * blockDim.x;
+  // per-Gaussian groups: xyz, f_dc, opacity, scaling, rotation
+  for (int64_t i = (int64_t)blockIdx.x * blockDim.x + threadIdx.x; i < P; i += stride) {
     const int g = (int)i;
     {  // xyz (group 0): the activated mean is the parameter itself
       const AdamScalars& s = s_sc[0];
@@ -363,20 +362,43 @@ __global__ void __launch_bounds__(256) adam_gaussian_kernel(const __grid_constan
       const float n2 = fmaxf(sqrtf(nr[0] * nr[0] + nr[1] * nr[1] + nr[2] * nr[2] + nr[3] * nr[3]), 1e-12f);
       for (int k = 0; k < 4; ++k) p.act.rotations[4 * g + k] = nr[k] / n2;
     }
-  } else {
-    // f_rest (group 2), elementwise: element e of Gaussian g's (M - 1) x 3 rest coefficients
-    // (rest_n < 2^32 is checked on the host, so 32-bit index arithmetic suffices)
-    const uint32_t e = (uint32_t)(i - P);
-    const uint32_t per = (uint32_t)(M - 1) * 3u;
-    const uint32_t g = e / per, r = e - g * per;
-    const AdamScalars& s = s_sc[2];
-    const size_t sh_idx = (size_t)g * M * 3 + 3 + r;
-    const float v = adam_update(p.prm.features_rest[e], p.st.m_rest[e], p.st.v_rest[e], p.dL_dsh[sh_idx], s);
-    if (p.act.shs_bf16)
-      reinterpret_cast<__nv_bfloat16*>(p.act.shs)[sh_idx] = __float2bfloat16_rn(v);
-    else
-      static_cast<float*>(p.act.shs)[sh_idx] = v;
   }
+  // f_rest (group 2), elementwise (element e of Gaussian g's (M - 1) x 3 rest coefficients; rest_n <
+  // 2^32 is checked on the host, so 32-bit index arithmetic suffices).  Each thread loads
+  // kAdamUnroll elements before updating any, so that many loads are in flight per thread.
+  constexpr int kAdamUnroll = 4;
+  const uint32_t per = (uint32_t)(M - 1) * 3u;
+  const AdamScalars& s = s_sc[2];
+  for (int64_t base = (int64_t)blockIdx.x * blockDim.x * kAdamUnroll + threadIdx.x; base < rest_n;
+       base += stride * kAdamUnroll) {
+    float pv[kAdamUnroll], mv[kAdamUnroll], vv[kAdamUnroll], gv[kAdamUnroll];
+    size_t sh_idx[kAdamUnroll];
+#pragma unroll
+    for (int u = 0; u < kAdamUnroll; ++u) {
+      const int64_t e = base + (int64_t)u * blockDim.x;
+      if (e < rest_n) {
+        const uint32_t g = (uint32_t)e / per, r = (uint32_t)e - g * per;
+        sh_idx[u] = (size_t)g * M * 3 + 3 + r;
+        pv[u] = p.prm.features_rest[e];
+        mv[u] = p.st.m_rest[e];
+        vv[u] = p.st.v_rest[e];
+        gv[u] = p.dL_dsh[sh_idx[u]];
+      }
+    }
+#pragma unroll
+    for (int u = 0; u < kAdamUnroll; ++u) {
+      const int64_t e = base + (int64_t)u * blockDim.x;
+      if (e < rest_n) {
+        const float v = adam_update(pv[u], mv[u], vv[u], gv[u], s);
+        p.prm.features_rest[e] = pv[u];
+        p.st.m_rest[e] = mv[u];
+        p.st.v_rest[e] = vv[u];
+        if (p.act.shs_bf16)
+          reinterpret_cast<__nv_bfloat16*>(p.act.shs)[sh_idx[u]] = __float2bfloat16_rn(v);
+        else
+          static_cast<float*>(p.act.shs)[sh_idx[u]] = v;
+      }
+    }
   }
 }
 
