@@ -11,10 +11,10 @@
 // 3 conic, 1 opacity, 3 colour) are not pushed with 9 global atomics per pixel as in the
 // reference (and the mean and conic terms are summed without their constant factors -W/2, -H/2,
 // -1/2, which the backward preprocess applies per Gaussian): a thread first sums them over its two
-// pixels, the warp that owns the 8 x 8 patch
-// reduces them with a reduce-scatter of 8 values (9 shuffles) plus a butterfly for the ninth, and
-// 8 lanes add one accumulator record per splat; when a single lane contributes it adds its 9
-// values directly.  Warps skip splats whose alpha-support box misses their patch or that lie
+// pixels and writes the 9 sums to its warp's shared buffer; every second contributing splat the
+// warp that owns the 8 x 8 patch reduces the buffer transposed (one lane per splat and value, 32
+// terms each) and adds the accumulator records with one atomic per value.  When a single lane
+// contributes it adds its 9 values directly.  Warps skip splats whose alpha-support box misses their patch or that lie
 // behind all of their pixels' last contributors, and the block starts at the batch holding its
 // largest last contributor instead of at the end of the range.
 #include "blend_common.cuh"
@@ -22,37 +22,30 @@
 namespace omnigs {
 namespace {
 
-// Sums v[0..8] over the warp and adds the totals to acc[0..8] (one accumulator record).
-__device__ __forceinline__ void warp_reduce_add9(const float v[9], float* acc, int lane) {
-  const bool b4 = lane & 16, b3 = lane & 8, b2 = lane & 4;
-  float a[4];
+// Per-warp buffer of the lane values of contributing splats: row 9 h + q holds value q of buffered
+// splat h for the 32 lanes.  The row stride of 36 floats puts the 16-byte reads of 8 consecutive
+// rows (one quarter-warp) on distinct banks; the lanes' writes of one row are consecutive words.
+constexpr int kRedStride = 36;
+
+// Adds the buffered splats' lane sums to their accumulator records: lane t sums row t over the
+// 32 lanes (eight 16-byte reads, packed adds) and adds the total with one atomic.
+__device__ __forceinline__ void flush_reduction(float (*red)[kRedStride], const uint32_t* gidx, int n,
+                                                float* grad_acc, int lane) {
+  __syncwarp();
+  for (int t = lane; t < n * 9; t += 32) {
+    const int h = t / 9, q = t - 9 * h;
+    const float4* row = reinterpret_cast<const float4*>(red[t]);
+    float2 s0 = make_float2(0.f, 0.f), s1 = s0;
 #pragma unroll
-  for (int i = 0; i < 4; ++i) {
-    const float send = b4 ? v[i] : v[i + 4];
-    const float keep = b4 ? v[i + 4] : v[i];
-    a[i] = keep + __shfl_xor_sync(kFullMask, send, 16);
+    for (int i = 0; i < 8; ++i) {
+      const float4 x = row[i];
+      s0 = add2(s0, make_float2(x.x, x.y));
+      s1 = add2(s1, make_float2(x.z, x.w));
+    }
+    s0 = add2(s0, s1);
+    atomicAdd(grad_acc + 12 * (size_t)gidx[h] + q, s0.x + s0.y);
   }
-  float b[2];
-#pragma unroll
-  for (int i = 0; i < 2; ++i) {
-    const float send = b3 ? a[i] : a[i + 2];
-    const float keep = b3 ? a[i + 2] : a[i];
-    b[i] = keep + __shfl_xor_sync(kFullMask, send, 8);
-  }
-  float c;
-  {
-    const float send = b2 ? b[0] : b[1];
-    const float keep = b2 ? b[1] : b[0];
-    c = keep + __shfl_xor_sync(kFullMask, send, 4);
-  }
-  c += __shfl_xor_sync(kFullMask, c, 2);
-  c += __shfl_xor_sync(kFullMask, c, 1);
-  float e = v[8];
-#pragma unroll
-  for (int o = 16; o > 0; o >>= 1) e += __shfl_xor_sync(kFullMask, e, o);
-  // lane 4k now holds the total of value k
-  if ((lane & 3) == 0) atomicAdd(acc + (lane >> 2), c);
-  if (lane == 0) atomicAdd(acc + 8, e);
+  __syncwarp();  // the rows are rewritten next
 }
 
 __device__ __forceinline__ float rcp_approx(float x) {
@@ -60,6 +53,9 @@ __device__ __forceinline__ float rcp_approx(float x) {
   asm("rcp.approx.ftz.f32 %0, %1;" : "=f"(r) : "f"(x));
   return r;
 }
+
+// Eight resident blocks per SM (at most 64 registers per thread) measured fastest on a B200.
+constexpr int kBlendBwdMinBlocks = 8;
 
 template <int kBatch, bool kWrap>
 __device__ __forceinline__ void blend_backward_tile(const TileJob& job, const BlendSource& src, float* grad_acc) {
@@ -69,6 +65,11 @@ __device__ __forceinline__ void blend_backward_tile(const TileJob& job, const Bl
   __shared__ float4 s_c[kBatch];
   __shared__ uint32_t s_g[kBatch];
   __shared__ uint32_t s_warp_last[kBlendWarps];
+  // Two buffered splats (18 rows: one flush round) measured fastest on a B200: larger buffers cost
+  // occupancy (shared memory, registers) faster than they save reduction instructions.
+  constexpr int kRedSplats = 2;
+  __shared__ __align__(16) float s_red[kBlendWarps][kRedSplats * 9][kRedStride];
+  __shared__ uint32_t s_red_g[kBlendWarps][kRedSplats];
   const BlendPatch patch = BlendPatch::make(job.tile_x, job.tile_y, job.wrap_w);
   const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
   const uint2 range = job.range;
@@ -100,6 +101,9 @@ __device__ __forceinline__ void blend_backward_tile(const TileJob& job, const Bl
   // colour of everything behind the current splat, accumulated back to front
   float2 acc0 = make_float2(0.f, 0.f), acc1 = acc0, acc2 = acc0;
   const float2 pyf = make_float2(patch.pyf(0), patch.pyf(1));
+
+  float(*red)[kRedStride] = s_red[threadIdx.x >> 5];
+  int nred = 0;  // buffered splats (warp-uniform)
 
   const uint32_t warp_last = __reduce_max_sync(kFullMask, max(lc[0], lc[1]));
   if (lane == 0) s_warp_last[warp] = warp_last;
@@ -184,23 +188,30 @@ __device__ __forceinline__ void blend_backward_tile(const TileJob& job, const Bl
         }
         const unsigned cm = __ballot_sync(kFullMask, contrib);
         if (cm == 0) continue;
-        float* acc = grad_acc + 12 * (size_t)s_g[jj];
         if ((cm & (cm - 1)) == 0) {  // one contributing lane: add its values directly
           if (contrib) {
+            float* acc = grad_acc + 12 * (size_t)s_g[jj];
 #pragma unroll
             for (int q = 0; q < 9; ++q) atomicAdd(acc + q, v[q]);
           }
         } else {
-          warp_reduce_add9(v, acc, lane);
+#pragma unroll
+          for (int q = 0; q < 9; ++q) red[nred * 9 + q][lane] = v[q];
+          if (lane == 0) s_red_g[warp][nred] = s_g[jj];
+          if (++nred == kRedSplats) {
+            flush_reduction(red, s_red_g[warp], nred, grad_acc, lane);
+            nred = 0;
+          }
         }
       }
     }
   }
+  if (nred) flush_reduction(red, s_red_g[warp], nred, grad_acc, lane);
 }
 
 // One view: block (x, y) back-propagates tile (x, y).
 template <int kBatch>
-__global__ void __launch_bounds__(kBlendThreads) render_backward_kernel(RenderParams p) {
+__global__ void __launch_bounds__(kBlendThreads, kBlendBwdMinBlocks) render_backward_kernel(RenderParams p) {
   TileJob job;
   job.tile_x = blockIdx.x;
   job.tile_y = blockIdx.y;
@@ -218,7 +229,7 @@ __global__ void __launch_bounds__(kBlendThreads) render_backward_kernel(RenderPa
 
 // All views of a batch in one launch: block b back-propagates global tile b.
 template <int kBatch, bool kWrap>
-__global__ void __launch_bounds__(kBlendThreads) batch_render_backward_kernel(const __grid_constant__ BatchRenderParams p) {
+__global__ void __launch_bounds__(kBlendThreads, kBlendBwdMinBlocks) batch_render_backward_kernel(const __grid_constant__ BatchRenderParams p) {
   const TileJob job = batch_tile_job(p, blockIdx.x);
   blend_backward_tile<kBatch, kWrap>(job, BlendSource{p.point_list, p.splat, p.color, (uint32_t)p.P * (uint32_t)p.V, p.capacity},
                       p.grad_acc);
