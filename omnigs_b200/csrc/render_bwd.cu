@@ -13,10 +13,10 @@
 // -1/2, which the backward preprocess applies per Gaussian): a thread first sums them over its two
 // pixels and writes the 9 sums to its warp's shared buffer; every second contributing splat the
 // warp that owns the 8 x 8 patch reduces the buffer transposed (one lane per splat and value, 32
-// terms each) and adds the accumulator records with one atomic per value.  When a single lane
-// contributes it adds its 9 values directly.  Warps skip splats whose alpha-support box misses their patch or that lie
-// behind all of their pixels' last contributors, and the block starts at the batch holding its
-// largest last contributor instead of at the end of the range.
+// terms each) and adds the accumulator records with one atomic per value.  Warps skip splats
+// whose alpha-support box misses their patch or that lie behind all of their pixels' last
+// contributors, and the block starts at the batch holding its largest last contributor instead of
+// at the end of the range.
 #include "blend_common.cuh"
 
 namespace omnigs {
@@ -165,43 +165,30 @@ __device__ __forceinline__ void blend_backward_tile(const TileJob& job, const Bl
             //   dL/d(conic) = -q (dx^2, dx dy, dy^2) / 2.
             // The per-pixel sums keep only q (a dx + b dy), ...; the constant factors -W/2, -H/2 and
             // -1/2 are applied once per Gaussian by the backward preprocess.
+            // The thread's two pixels share dx, so the sums over them factor through
+            // sum q, sum q dy and sum q dy^2.
             const float2 w5 = mul2(Ge, dLda);
             const float2 q = mul2(f2(b.y), w5);
-            const float2 w0 = mul2(q, fma2(f2(a.w), dy, f2(__fmul_rn(a.z, dx))));
-            const float2 w1 = mul2(q, fma2(f2(b.x), dy, f2(__fmul_rn(a.w, dx))));
-            const float2 w2 = mul2(q, f2(dx * dx));
-            const float2 w3 = mul2(q, mul2(f2(dx), dy));
-            const float2 w4 = mul2(q, mul2(dy, dy));
-            const float2 w6 = mul2(dcd, dp0);
-            const float2 w7 = mul2(dcd, dp1);
-            const float2 w8 = mul2(dcd, dp2);
-            v[0] = w0.x + w0.y;
-            v[1] = w1.x + w1.y;
-            v[2] = w2.x + w2.y;
-            v[3] = w3.x + w3.y;
-            v[4] = w4.x + w4.y;
+            const float2 qy = mul2(q, dy);
+            const float qs = q.x + q.y, qdy = qy.x + qy.y;
+            v[0] = fmaf(a.z * dx, qs, a.w * qdy);
+            v[1] = fmaf(a.w * dx, qs, b.x * qdy);
+            v[2] = dx * dx * qs;
+            v[3] = dx * qdy;
+            v[4] = fmaf(qy.x, dy.x, qy.y * dy.y);
             v[5] = w5.x + w5.y;
-            v[6] = w6.x + w6.y;
-            v[7] = w7.x + w7.y;
-            v[8] = w8.x + w8.y;
+            v[6] = fmaf(dcd.x, dp0.x, dcd.y * dp0.y);
+            v[7] = fmaf(dcd.x, dp1.x, dcd.y * dp1.y);
+            v[8] = fmaf(dcd.x, dp2.x, dcd.y * dp2.y);
           }
         }
-        const unsigned cm = __ballot_sync(kFullMask, contrib);
-        if (cm == 0) continue;
-        if ((cm & (cm - 1)) == 0) {  // one contributing lane: add its values directly
-          if (contrib) {
-            float* acc = grad_acc + 12 * (size_t)s_g[jj];
+        if (!__any_sync(kFullMask, contrib)) continue;
 #pragma unroll
-            for (int q = 0; q < 9; ++q) atomicAdd(acc + q, v[q]);
-          }
-        } else {
-#pragma unroll
-          for (int q = 0; q < 9; ++q) red[nred * 9 + q][lane] = v[q];
-          if (lane == 0) s_red_g[warp][nred] = s_g[jj];
-          if (++nred == kRedSplats) {
-            flush_reduction(red, s_red_g[warp], nred, grad_acc, lane);
-            nred = 0;
-          }
+        for (int q = 0; q < 9; ++q) red[nred * 9 + q][lane] = v[q];
+        if (lane == 0) s_red_g[warp][nred] = s_g[jj];
+        if (++nred == kRedSplats) {
+          flush_reduction(red, s_red_g[warp], nred, grad_acc, lane);
+          nred = 0;
         }
       }
     }
