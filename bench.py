@@ -70,6 +70,71 @@ def dist_env():
 
 
 # ---------------------------------------------------------------- clocks -----------------------
+class NvmlClockSampler:
+    """Samples SM clock and clock-event (throttle) reasons through NVML every 5 ms while running
+    (read-only queries), so that even a timed region of a few tens of milliseconds gets samples."""
+
+    REASONS = (("hw_slowdown", "nvmlClocksEventReasonHwSlowdown"),
+               ("hw_thermal_slowdown", "nvmlClocksEventReasonHwThermalSlowdown"),
+               ("sw_thermal_slowdown", "nvmlClocksEventReasonSwThermalSlowdown"),
+               ("sw_power_cap", "nvmlClocksEventReasonSwPowerCap"))
+
+    def __init__(self, gpu_uuid: str):
+        import pynvml
+
+        self.nvml = pynvml
+        pynvml.nvmlInit()
+        self.handle = pynvml.nvmlDeviceGetHandleByUUID(gpu_uuid)
+        self.max_mhz = float(pynvml.nvmlDeviceGetMaxClockInfo(self.handle, pynvml.NVML_CLOCK_SM))
+        self.samples, self.stop = [], threading.Event()
+
+    def _poll(self):
+        n = self.nvml
+        while not self.stop.is_set():
+            try:
+                mhz = float(n.nvmlDeviceGetClockInfo(self.handle, n.NVML_CLOCK_SM))
+                bits = int(n.nvmlDeviceGetCurrentClocksEventReasons(self.handle))
+                self.samples.append((mhz, bits))
+            except n.NVMLError:
+                pass
+            self.stop.wait(0.005)
+
+    def __enter__(self):
+        self._poll_once()
+        self.thread = threading.Thread(target=self._poll, daemon=True)
+        self.thread.start()
+        return self
+
+    def _poll_once(self):
+        n = self.nvml
+        self.samples.append((float(n.nvmlDeviceGetClockInfo(self.handle, n.NVML_CLOCK_SM)),
+                             int(n.nvmlDeviceGetCurrentClocksEventReasons(self.handle))))
+
+    def __exit__(self, *exc):
+        self.stop.set()
+        self.thread.join(timeout=5)
+        self._poll_once()
+
+    def summary(self) -> dict:
+        reasons = set()
+        for _, bits in self.samples:
+            for name, attr in self.REASONS:
+                if bits & getattr(self.nvml, attr):
+                    reasons.add(name)
+        return {"sm_mhz": statistics.median(m for m, _ in self.samples), "sm_max_mhz": self.max_mhz,
+                "reasons": sorted(reasons), "samples": len(self.samples), "source": "nvml, 5 ms"}
+
+
+def clock_sampler(gpu_uuid: str | None):
+    """NVML sampler when NVML answers, else nvidia-smi at its 200 ms interval."""
+    if gpu_uuid:
+        try:
+            return NvmlClockSampler(gpu_uuid)
+        except Exception:
+            pass
+    return ClockSampler(gpu_uuid)
+
+
 class ClockSampler:
     """Samples SM clock and throttle reasons with nvidia-smi while running."""
 
@@ -122,7 +187,7 @@ class ClockSampler:
         if not sm:
             return {"sm_mhz": None, "sm_max_mhz": None, "reasons": ["unavailable"], "samples": 0}
         return {"sm_mhz": statistics.median(sm), "sm_max_mhz": max(mx), "reasons": sorted(reasons),
-                "samples": len(sm)}
+                "samples": len(sm), "source": "nvidia-smi, 200 ms"}
 
 
 # ---------------------------------------------------------------- roofline ---------------------
@@ -489,7 +554,7 @@ def run_omnigs(args, rank, world, local_rank):
         dist.barrier()
     torch.cuda.synchronize()
     launches0 = capi.kernel_launches()
-    with ClockSampler(gpu_uuid) as clocks:
+    with clock_sampler(gpu_uuid) as clocks:
         ev0.record(stream)
         for _ in range(args.steps):
             step()
