@@ -16,7 +16,7 @@ import math
 import numpy as np
 import torch
 
-from . import batch, capi, sharding
+from . import batch, capi, ply, sharding
 from .lonlat import GaussianTensors
 
 # learning rates of the reference's lonlat configurations (cfg/lonlat/*.yaml: Optimization.*),
@@ -83,6 +83,21 @@ class GaussianModelState:
         return GaussianModelState(t(g.means3D), t(g.shs[:, :1]), t(g.shs[:, 1:]),
                                   t(np.log(op / (1 - op)).astype(np.float32)),
                                   t(np.log(g.scales).astype(np.float32)), t(g.rotations), sh_bf16=sh_bf16, **kw)
+
+    @staticmethod
+    def from_ply(path: str, device="cuda", sh_bf16: bool = False, **kw) -> "GaussianModelState":
+        """From a scene saved by the reference's savePly (raw parameters; gaussian_model.cpp:860)."""
+        g = ply.read_ply(path)
+        t = lambda a: torch.from_numpy(np.ascontiguousarray(a)).to(device)  # noqa: E731
+        return GaussianModelState(t(g.xyz), t(g.features_dc), t(g.features_rest), t(g.opacity), t(g.scaling),
+                                  t(g.rotation), sh_bf16=sh_bf16, **kw)
+
+    def save_ply(self, path: str) -> None:
+        """Writes the raw parameters in the reference's PLY layout (gaussian_model.cpp:978)."""
+        n = lambda x: x.detach().cpu().numpy()  # noqa: E731
+        ply.write_ply(path, ply.PlyGaussians(xyz=n(self.xyz), features_dc=n(self.features_dc),
+                                             features_rest=n(self.features_rest), opacity=n(self.opacity),
+                                             scaling=n(self.scaling), rotation=n(self.rotation)))
 
     def _structs(self):
         prm = capi.GaussianParams()

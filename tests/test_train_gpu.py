@@ -124,3 +124,35 @@ def test_captured_train_steps_reduce_the_loss(cuda, sh_bf16):
     assert math.isfinite(last) and last < 0.8 * first, (first, last)
     assert float(stepper.grads.denom.max()) > 0
     assert model.step_count == 61
+
+
+def test_ply_scene_loads_into_the_model_and_saves_back(cuda, tmp_path):
+    """A scene in the reference's PLY layout loads into GaussianModelState (activated values as the
+    model's activations define them), renders, and saves back after an Adam step with the updated
+    raw parameters."""
+    from omnigs_b200 import ply
+
+    g = scenes.make_gaussians(2000, seed=11)
+    src = train.GaussianModelState.from_activated(g, device=cuda)
+    path = str(tmp_path / "scene.ply")
+    src.save_ply(path)
+    m = train.GaussianModelState.from_ply(path, device=cuda)
+    for a, b in zip(m.params, src.params):
+        assert torch.equal(a, b)
+    t, ts = m.tensors(), src.tensors()
+    for k in ("means3D", "opacities", "scales", "rotations", "shs"):
+        assert torch.equal(getattr(t, k), getattr(ts, k)), k
+    a = ply.read_ply(path).activated()
+    torch.testing.assert_close(t.scales.cpu(), torch.from_numpy(a.scales), rtol=1e-6, atol=0)
+    torch.testing.assert_close(t.opacities.cpu(), torch.from_numpy(a.opacities), rtol=1e-6, atol=0)
+    torch.testing.assert_close(t.rotations.cpu(), torch.from_numpy(a.rotations), rtol=1e-6, atol=1e-7)
+    # one step with unit gradients moves every raw parameter; the saved file holds the new values
+    ones = lambda *s: torch.ones(*s, device=cuda)  # noqa: E731
+    m.adam_step(ones(m.P, 3), ones(m.P, m.M, 3), ones(m.P, 1), ones(m.P, 3), ones(m.P, 4))
+    torch.cuda.synchronize()
+    path2 = str(tmp_path / "step.ply")
+    m.save_ply(path2)
+    h = ply.read_ply(path2)
+    np.testing.assert_array_equal(h.xyz, m.xyz.cpu().numpy())
+    np.testing.assert_array_equal(h.features_rest, m.features_rest.cpu().numpy())
+    assert not np.array_equal(h.xyz, ply.read_ply(path).xyz)
