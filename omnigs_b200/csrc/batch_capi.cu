@@ -268,20 +268,16 @@ int omnigs_batch_render(const OmnigsBatchArgs* a, void* state, size_t state_byte
     d.gy[v] = bp.views[v].gy;
     d.tile_base[v] = bp.views[v].tile_base;
   }
+  d.hist = thist + kDepthPasses * kRadix;
+  d.hist_passes = td.passes;
+  for (int q = 0; q < td.passes; ++q) {
+    d.hist_shift[q] = td.shift[q];
+    d.hist_mask[q] = td.mask[q];
+  }
   staged(OMNIGS_STAGE_DUPLICATE, 1, s, [&] { launch_duplicate(d, s); });
 
   // 3. stable tile sort of all instances
-  HistParams ht{};
-  ht.keys = tkeys[0];
-  ht.count_hdr = hdr;
-  ht.capacity = capacity;
-  ht.passes = td.passes;
-  for (int q = 0; q < td.passes; ++q) {
-    ht.shift[q] = td.shift[q];
-    ht.mask[q] = td.mask[q];
-  }
-  ht.hist = thist + kDepthPasses * kRadix;
-  staged(OMNIGS_STAGE_SORT, 1, s, [&] { launch_histogram(ht, capacity, s); });
+  // (its digit histograms were counted by the duplicate pass)
   for (int q = 0; q < td.passes; ++q) {
     OnesweepParams op{};
     op.keys_in = tkeys[q & 1];

@@ -9,7 +9,8 @@
 //  1. depth sort: a stable LSD radix sort (4 onesweep passes of 8 bits) of the P Gaussians by the
 //     bits of their depth, i.e. the order (depth bits, index);
 //  2. duplicate: instances are emitted walking the Gaussians in that order, each block scanning
-//     its Gaussians' tile counts and joining a decoupled look-back for its output offset;
+//     its Gaussians' tile counts and joining a decoupled look-back for its output offset, and
+//     counting the digits of the keys it writes for the tile sort;
 //  3. tile sort: a stable LSD radix sort (2 onesweep passes) of the instances by tile id only.
 // Stability makes (1)+(3) equal to the reference's single sort: instance passes drop from six
 // over 12-byte items to two over 8-byte items; the four depth passes run over P, not R, items.
@@ -45,6 +46,19 @@ __device__ __forceinline__ uint32_t item_count(const GeomHeader* count_hdr, uint
 }
 
 // ---------------------------------------------------------------- digit histograms ------------
+// Adds the warp's digits (lanes in `live`, a prefix of the warp) to a shared histogram.  Keys of a
+// sort are either spread over many digits (per-lane atomics rarely collide) or nearly constant
+// within a warp (the top digit of depth bits): when every live lane holds lane 0's digit, lane 0
+// adds the whole count with one atomic.
+__device__ __forceinline__ void count_digit(uint32_t* hist, uint32_t digit, bool valid, unsigned live, int lane) {
+  const uint32_t d0 = __shfl_sync(kFullMask, digit, 0);
+  if (__all_sync(kFullMask, !valid || digit == d0)) {
+    if (lane == 0 && live) atomicAdd(&hist[d0], (uint32_t)__popc(live));
+  } else if (valid) {
+    atomicAdd(&hist[digit], 1u);
+  }
+}
+
 constexpr int kHistUnroll = 4;  // keys per thread loaded before any of them is counted
 
 __global__ void __launch_bounds__(256) histogram_kernel(const __grid_constant__ HistParams p) {
@@ -55,7 +69,7 @@ __global__ void __launch_bounds__(256) histogram_kernel(const __grid_constant__ 
   const size_t seg_base = (size_t)blockIdx.y * n;  // gridDim.y segments
   const int lane = threadIdx.x & 31;
   const uint32_t stride = gridDim.x * blockDim.x;
-  // Whole warps iterate together so that match.any sees all 32 lanes; each thread first loads
+  // Whole warps iterate together (the counting votes over the warp); each thread first loads
   // kHistUnroll keys (independent loads in flight), then counts them.
   for (uint32_t base = blockIdx.x * blockDim.x + (threadIdx.x & ~31u); base < n; base += stride * kHistUnroll) {
     uint32_t key[kHistUnroll];
@@ -66,15 +80,15 @@ __global__ void __launch_bounds__(256) histogram_kernel(const __grid_constant__ 
       valid[u] = i < n;
       key[u] = valid[u] ? p.keys[seg_base + i] : 0u;
     }
+    unsigned live[kHistUnroll];
+#pragma unroll
+    for (int u = 0; u < kHistUnroll; ++u) live[u] = __ballot_sync(kFullMask, valid[u]);
 #pragma unroll
     for (int q = 0; q < kDepthPasses; ++q) {
       if (q >= p.passes) break;
 #pragma unroll
-      for (int u = 0; u < kHistUnroll; ++u) {
-        const uint32_t digit = (key[u] >> p.shift[q]) & p.mask[q];
-        const unsigned peers = __match_any_sync(kFullMask, valid[u] ? digit : (0x10000u | lane));
-        if (valid[u] && lane == __ffs(peers) - 1) atomicAdd(&s_hist[q][digit], (uint32_t)__popc(peers));
-      }
+      for (int u = 0; u < kHistUnroll; ++u)
+        count_digit(s_hist[q], (key[u] >> p.shift[q]) & p.mask[q], valid[u], live[u], lane);
     }
   }
   __syncthreads();
@@ -269,7 +283,8 @@ __global__ void __launch_bounds__(kSortThreads, 3) onesweep_kernel(OnesweepParam
 }
 
 // ---------------------------------------------------------------- duplicate -------------------
-// duplicateWithKeys over the depth-sorted Gaussians, fused with the scan of their tile counts.
+// duplicateWithKeys over the depth-sorted Gaussians, fused with the scan of their tile counts and
+// with the digit histograms of the tile sort that follows.
 // Block b takes sorted positions [256 b, 256 b + 256); its output offset comes from a block scan
 // plus a decoupled look-back over the preceding blocks.  Each warp then writes the instances of
 // its 32 Gaussians (one contiguous span) 32 at a time: a 5-step shuffle search finds each
@@ -278,11 +293,13 @@ __global__ void __launch_bounds__(kScanBlock) duplicate_kernel(const __grid_cons
   __shared__ uint32_t s_tile;
   __shared__ uint32_t s_warp[kScanBlock / 32];
   __shared__ unsigned long long s_excl;
+  __shared__ uint32_t s_hist[kTilePasses][kRadix];
   if (!instances_fit(p.hdr, p.capacity)) {
     if (blockIdx.x == 0 && threadIdx.x == 0) atomicOr(&p.hdr->status, kStatusCapacity);
     return;
   }
   if (threadIdx.x == 0) s_tile = atomicAdd(&p.hdr->dup_tile_counter, 1u);
+  for (int k = threadIdx.x; k < kTilePasses * kRadix; k += kScanBlock) (&s_hist[0][0])[k] = 0;
   __syncthreads();
   const uint32_t tile = s_tile;
   const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
@@ -399,15 +416,29 @@ __global__ void __launch_bounds__(kScanBlock) duplicate_kernel(const __grid_cons
     const int o_width = __shfl_sync(kFullMask, width, pos);
     const int o_col0 = __shfl_sync(kFullMask, col0, pos);
     const uint32_t o_g = __shfl_sync(kFullMask, g, pos);
-    if (o < w_end && o < limit) {
+    const bool ok = o < w_end && o < limit;
+    uint32_t key = 0;
+    if (ok) {
       const uint32_t local = o - o_start;
       const uint32_t ry = local / (uint32_t)o_width;
       int tx = o_col0 + (int)(local - ry * (uint32_t)o_width);
       if (tx < 0) tx += o_pitch;  // seam wrap: columns left of 0 or right of gx - 1
       if (tx >= o_pitch) tx -= o_pitch;
-      p.tkeys[o] = o_origin + ry * (uint32_t)o_pitch + (uint32_t)tx;
+      key = o_origin + ry * (uint32_t)o_pitch + (uint32_t)tx;
+      p.tkeys[o] = key;
       p.tvals[o] = o_g;
     }
+    // digit histograms of the tile sort (the pass that would otherwise re-read every key)
+    const unsigned live = __ballot_sync(kFullMask, ok);
+#pragma unroll
+    for (int q = 0; q < kTilePasses; ++q)
+      if (q < p.hist_passes) count_digit(s_hist[q], (key >> p.hist_shift[q]) & p.hist_mask[q], ok, live, lane);
+  }
+  if (p.hist_passes == 0) return;
+  __syncthreads();
+  for (int k = threadIdx.x; k < p.hist_passes * kRadix; k += kScanBlock) {
+    const uint32_t c = (&s_hist[0][0])[k];
+    if (c) atomicAdd(&p.hist[k], c);
   }
 }
 

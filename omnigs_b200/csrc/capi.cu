@@ -277,20 +277,16 @@ int omnigs_lonlat_render(const OmnigsLonlatForwardArgs* a, void* geom, size_t ge
   d.scan_state = at<unsigned long long>(geom, GL.dup_scan);
   d.capacity = capacity;
   d.hdr = hdr;
+  d.hist = hist + kDepthPasses * kRadix;
+  d.hist_passes = td.passes;
+  for (int q = 0; q < td.passes; ++q) {
+    d.hist_shift[q] = td.shift[q];
+    d.hist_mask[q] = td.mask[q];
+  }
   staged(OMNIGS_STAGE_DUPLICATE, 1, s, [&] { launch_duplicate(d, s); });
 
   // 3. stable tile sort of the instances
-  HistParams ht{};
-  ht.keys = tkeys[0];
-  ht.count_hdr = hdr;
-  ht.capacity = capacity;
-  ht.passes = td.passes;
-  for (int q = 0; q < td.passes; ++q) {
-    ht.shift[q] = td.shift[q];
-    ht.mask[q] = td.mask[q];
-  }
-  ht.hist = hist + kDepthPasses * kRadix;
-  staged(OMNIGS_STAGE_SORT, 1, s, [&] { launch_histogram(ht, capacity, s); });
+  // (its digit histograms were counted by the duplicate pass)
   for (int q = 0; q < td.passes; ++q) {
     OnesweepParams op{};
     op.keys_in = tkeys[q & 1];

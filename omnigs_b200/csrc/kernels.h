@@ -85,6 +85,12 @@ struct DuplicateParams {
   int seam_wrap;               // tile columns wrap modulo gx (rects from tile_rect_cyclic)
   int gx[kMaxBatchViews], gy[kMaxBatchViews];
   uint32_t tile_base[kMaxBatchViews];
+  // digit histograms of the tile sort, accumulated into hist[hist_passes][kRadix] (zeroed by the
+  // caller); hist_passes 0 counts nothing
+  uint32_t* hist;
+  int hist_passes;
+  int hist_shift[kTilePasses];
+  uint32_t hist_mask[kTilePasses];
 };
 
 struct RangesParams {
