@@ -11,8 +11,9 @@
 //  * for each staged batch a warp ballots which splats' alpha-support boxes (computed in the
 //    preprocess) touch its patch and iterates only over those, so pairs that the reference rejects
 //    pixel by pixel are skipped a warp at a time;
-//  * a warp stops as soon as all of its pixels are saturated (warp vote), and the block stops when
-//    every warp has (block vote), as in the reference;
+//  * a warp stops after the group of 32 candidate splats in which all of its pixels saturated
+//    (one warp vote per group; saturated pixels skip the per-splat work at once), and the block
+//    stops when every warp has (block vote), as in the reference;
 //  * splat geometry and colour are staged together (three float4 per instance) so the inner loop
 //    reads only shared memory.
 #include "blend_common.cuh"
@@ -84,11 +85,8 @@ __device__ __forceinline__ void blend_forward_tile(const TileJob& job, const Ble
             lc1 = act1 ? idx : lc1;
           }
         }
-        if (__all_sync(kFullMask, done0 && done1)) {
-          warp_done = true;
-          break;
-        }
       }
+      warp_done = __all_sync(kFullMask, done0 && done1);
     }
   }
 
