@@ -645,8 +645,9 @@ def run_omnigs(args, rank, world, local_rank):
             n, color, rad, gb, bb, ib = ext.rasterize_gaussians_cuda(
                 d_bg, gt.means3D, empty, gt.opacities, gt.scales, gt.rotations, 1.0, empty, d_view, d_view,
                 0.0, 0.0, H, W, gt.shs, 3, d_campos, False, 3, False)
-            # the forward returned after synchronising the compute stream, so step k-1's backward (the
-            # last reader of the other slot) is done: prefetch step k+1's inputs into it
+            # the forward returned once this step's binning had run on the compute stream, which
+            # follows step k-1's backward (the last reader of the other slot): prefetch step k+1's
+            # inputs into it
             if not last:
                 h2d(k + 1)
             img_ready = torch.cuda.Event()

@@ -16,10 +16,10 @@
  *
  * The three state buffers (geometry, binning, image) are caller-owned device memory whose sizes
  * come from the *_bytes queries; their layout is private to this library.  Nothing here allocates
- * device memory and nothing synchronises the host except omnigs_lonlat_read_status.  The instance
- * count (num_rendered) is produced and consumed on the device; the binning buffer is sized for a
- * caller-chosen capacity and a pass that would exceed it does no binning work and reports
- * OMNIGS_STATUS_CAPACITY through the status word.
+ * device memory and nothing synchronises the host except omnigs_lonlat_read_status and
+ * omnigs_lonlat_forward_early_status.  The instance count (num_rendered) is produced and consumed
+ * on the device; the binning buffer is sized for a caller-chosen capacity and a pass that would
+ * exceed it does no binning work and reports OMNIGS_STATUS_CAPACITY through the status word.
  *
  * Return codes: 0 on success, otherwise one of OMNIGS_ERR_*; omnigs_last_error() gives a message
  * (thread-local).  Kernels never trap: device-side failures are bits of the status word.
@@ -150,6 +150,19 @@ int omnigs_lonlat_forward(const OmnigsLonlatForwardArgs* args, void* geom, size_
  * array: calls that overlap on the GPU race and must not be issued. */
 int omnigs_lonlat_forward_noalloc(const OmnigsLonlatForwardArgs* args, int* num_rendered,
                                   omnigs_stream_t stream);
+
+/* omnigs_lonlat_forward that also returns num_rendered and the status word (what
+ * omnigs_lonlat_read_status gives), waiting only until the binning stage has run rather than for
+ * the whole stream: the forward blend is still executing on `stream` when it returns, so the
+ * caller's next launches overlap it.  Used by the LibTorch layer, whose RasterizeGaussiansCUDA
+ * returns num_rendered by value (src/rasterize_points.cu:163; the reference copies it to the host
+ * mid-pass, rasterizer_impl.cu:627-628).  The header is copied into pinned host memory that the
+ * library creates on a thread's first call on a device (with an event) and keeps until exit; the
+ * wait makes the call unsuitable for stream capture. */
+int omnigs_lonlat_forward_early_status(const OmnigsLonlatForwardArgs* args, void* geom, size_t geom_bytes,
+                                       void* binning, size_t binning_bytes, void* image,
+                                       size_t image_bytes, int* num_rendered, uint32_t* status,
+                                       omnigs_stream_t stream);
 
 /* Waits for `stream` and copies num_rendered and the status word to the host.  The one call that
  * synchronises; the reference's forward returns num_rendered by value (rasterizer.h:104). */

@@ -126,7 +126,8 @@ class TuneResult(ctypes.Structure):
 EXPORTED = ["omnigs_version", "omnigs_last_error", "omnigs_lonlat_geom_bytes",
             "omnigs_lonlat_image_bytes", "omnigs_lonlat_binning_bytes",
             "omnigs_lonlat_binning_capacity", "omnigs_lonlat_preprocess", "omnigs_lonlat_render",
-            "omnigs_lonlat_forward", "omnigs_lonlat_forward_noalloc", "omnigs_lonlat_read_status",
+            "omnigs_lonlat_forward", "omnigs_lonlat_forward_noalloc", "omnigs_lonlat_forward_early_status",
+            "omnigs_lonlat_read_status",
             "omnigs_lonlat_backward",
             "omnigs_mark_visible", "omnigs_timing_enable", "omnigs_timing_read",
             "omnigs_kernel_launches", "omnigs_lonlat_geom_view", "omnigs_lonlat_binning_view",
@@ -161,6 +162,9 @@ def lib() -> ctypes.CDLL:
         L.omnigs_lonlat_render.argtypes = fw + [_vp, ctypes.c_size_t, _vp, ctypes.c_size_t, _vp]
         L.omnigs_lonlat_forward.argtypes = fw + [_vp, ctypes.c_size_t, _vp, ctypes.c_size_t, _vp]
         L.omnigs_lonlat_forward_noalloc.argtypes = [ctypes.POINTER(ForwardArgs), ctypes.POINTER(_i), _vp]
+        L.omnigs_lonlat_forward_early_status.argtypes = fw + [_vp, ctypes.c_size_t, _vp, ctypes.c_size_t,
+                                                              ctypes.POINTER(_i), ctypes.POINTER(ctypes.c_uint32),
+                                                              _vp]
         L.omnigs_lonlat_read_status.argtypes = [_vp, ctypes.POINTER(_i),
                                                 ctypes.POINTER(ctypes.c_uint32), _vp]
         L.omnigs_lonlat_backward.argtypes = [ctypes.POINTER(BackwardArgs), _vp, ctypes.c_size_t,

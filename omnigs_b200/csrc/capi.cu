@@ -188,10 +188,42 @@ int omnigs_lonlat_preprocess(const OmnigsLonlatForwardArgs* a, void* geom, size_
   return check_launch("preprocess");
 }
 
-int omnigs_lonlat_render(const OmnigsLonlatForwardArgs* a, void* geom, size_t geom_bytes,
-                         void* binning, size_t binning_bytes, void* image, size_t image_bytes,
-                         omnigs_stream_t stream) {
-  g_last_error.clear();
+namespace {
+
+// Pinned host copy of the geometry header and the event recorded after the copy, one per host
+// thread and device, for omnigs_lonlat_forward_early_status.  Created on first use and kept for
+// the life of the process.
+struct EarlyStatus {
+  GeomHeader* host = nullptr;
+  cudaEvent_t copied = nullptr;
+};
+
+EarlyStatus* early_status_slot() {
+  int dev = 0;
+  if (cudaGetDevice(&dev) != cudaSuccess) return nullptr;
+  thread_local std::vector<EarlyStatus> slots;
+  if ((int)slots.size() <= dev) slots.resize(dev + 1);
+  EarlyStatus& e = slots[dev];
+  if (e.host == nullptr) {
+    if (cudaHostAlloc(reinterpret_cast<void**>(&e.host), sizeof(GeomHeader), cudaHostAllocDefault) != cudaSuccess) {
+      e.host = nullptr;
+      return nullptr;
+    }
+    if (cudaEventCreateWithFlags(&e.copied, cudaEventDisableTiming) != cudaSuccess) {
+      cudaFreeHost(e.host);
+      e.host = nullptr;
+      return nullptr;
+    }
+  }
+  return &e;
+}
+
+// Binning + forward blend.  With `early`, the header (instance count, status word; final once the
+// binning kernels have run) is copied to early->host and early->copied recorded between the binning
+// and the blend.
+int render_impl(const OmnigsLonlatForwardArgs* a, void* geom, size_t geom_bytes, void* binning,
+                size_t binning_bytes, void* image, size_t image_bytes, omnigs_stream_t stream,
+                EarlyStatus* early) {
   if (int rc = validate_forward(a)) return rc;
   cudaStream_t s = reinterpret_cast<cudaStream_t>(stream);
   const int64_t HW = (int64_t)a->W * a->H;
@@ -331,8 +363,22 @@ int omnigs_lonlat_render(const OmnigsLonlatForwardArgs* a, void* geom, size_t ge
   r.out_color = a->out_color;
   r.final_T = at<float>(image, IL.final_T);
   r.n_contrib = at<uint32_t>(image, IL.n_contrib);
+  if (early != nullptr) {
+    if (cudaMemcpyAsync(early->host, hdr, sizeof(GeomHeader), cudaMemcpyDeviceToHost, s) != cudaSuccess ||
+        cudaEventRecord(early->copied, s) != cudaSuccess)
+      return check_launch("copy status");
+  }
   staged(OMNIGS_STAGE_RENDER_FORWARD, 1, s, [&] { launch_render_forward(r, s); });
   return check_launch("render forward");
+}
+
+}  // namespace
+
+int omnigs_lonlat_render(const OmnigsLonlatForwardArgs* a, void* geom, size_t geom_bytes,
+                         void* binning, size_t binning_bytes, void* image, size_t image_bytes,
+                         omnigs_stream_t stream) {
+  g_last_error.clear();
+  return render_impl(a, geom, geom_bytes, binning, binning_bytes, image, image_bytes, stream, nullptr);
 }
 
 int omnigs_lonlat_forward(const OmnigsLonlatForwardArgs* a, void* geom, size_t geom_bytes,
@@ -340,6 +386,28 @@ int omnigs_lonlat_forward(const OmnigsLonlatForwardArgs* a, void* geom, size_t g
                           omnigs_stream_t stream) {
   if (int rc = omnigs_lonlat_preprocess(a, geom, geom_bytes, stream)) return rc;
   return omnigs_lonlat_render(a, geom, geom_bytes, binning, binning_bytes, image, image_bytes, stream);
+}
+
+int omnigs_lonlat_forward_early_status(const OmnigsLonlatForwardArgs* a, void* geom, size_t geom_bytes,
+                                       void* binning, size_t binning_bytes, void* image, size_t image_bytes,
+                                       int* num_rendered, uint32_t* status, omnigs_stream_t stream) {
+  if (num_rendered == nullptr || status == nullptr)
+    return fail(OMNIGS_ERR_INVALID_ARGUMENT, "num_rendered and status must not be NULL");
+  if (int rc = omnigs_lonlat_preprocess(a, geom, geom_bytes, stream)) return rc;
+  g_last_error.clear();
+  if (a->P == 0) {
+    *num_rendered = 0;
+    *status = 0;
+    return render_impl(a, geom, geom_bytes, binning, binning_bytes, image, image_bytes, stream, nullptr);
+  }
+  EarlyStatus* e = early_status_slot();
+  if (e == nullptr) return fail(OMNIGS_ERR_CUDA, "could not create the pinned status slot");
+  if (int rc = render_impl(a, geom, geom_bytes, binning, binning_bytes, image, image_bytes, stream, e)) return rc;
+  if (cudaEventSynchronize(e->copied) != cudaSuccess) return check_launch("wait for the binning status");
+  const unsigned long long n = e->host->num_rendered64;
+  *num_rendered = (int)(n > 0x7fffffffull ? 0x7fffffff : n);
+  *status = e->host->status;
+  return OMNIGS_OK;
 }
 
 int omnigs_lonlat_read_status(const void* geom, int* num_rendered, uint32_t* status,

@@ -4,8 +4,9 @@
 //  * all launches go to the current CUDA stream of the input's device;
 //  * the binning buffer is sized from a capacity hint (the previous call's instance count, or a
 //    per-Gaussian estimate), so the pipeline runs without the reference's mid-pass device-to-host
-//    copy; the one host sync reads num_rendered (which this API returns by value) at the end, and
-//    only when the hint was too small is the binning stage resized and re-run;
+//    copy; the one host wait reads num_rendered (which this API returns by value) once the
+//    binning has run, while the blend still runs, and only when the hint was too small is the
+//    binning stage resized and re-run;
 //  * gradient outputs are allocated uninitialised because the backward writes every element.
 #include "rasterize_points.h"
 
@@ -112,11 +113,13 @@ RasterizeGaussiansCUDA(const torch::Tensor& background, const torch::Tensor& mea
     const int64_t capacity = std::max<int64_t>(g_capacity_hint.load(), 4 * (int64_t)P);
     binningBuffer.resize_({(int64_t)omnigs_lonlat_binning_bytes(capacity)});
     auto s = reinterpret_cast<omnigs_stream_t>(stream);
-    check_rc(omnigs_lonlat_forward(&a, geomBuffer.data_ptr(), geomBuffer.numel(), binningBuffer.data_ptr(),
-                                   binningBuffer.numel(), imgBuffer.data_ptr(), imgBuffer.numel(), s),
-             "forward");
+    // returns once the binning has run (num_rendered and the status are final); the blend is still
+    // running on the stream, so the caller's next launches overlap it
     uint32_t status = 0;
-    check_rc(omnigs_lonlat_read_status(geomBuffer.data_ptr(), &rendered, &status, s), "read status");
+    check_rc(omnigs_lonlat_forward_early_status(&a, geomBuffer.data_ptr(), geomBuffer.numel(),
+                                                binningBuffer.data_ptr(), binningBuffer.numel(),
+                                                imgBuffer.data_ptr(), imgBuffer.numel(), &rendered, &status, s),
+             "forward");
     if (status & OMNIGS_STATUS_CAPACITY) {
       binningBuffer.resize_({(int64_t)omnigs_lonlat_binning_bytes(rendered)});
       check_rc(omnigs_lonlat_render(&a, geomBuffer.data_ptr(), geomBuffer.numel(), binningBuffer.data_ptr(),

@@ -129,6 +129,22 @@ class LonlatState:
             capi.stream_handle(stream))
         capi.check(rc, "omnigs_lonlat_forward")
 
+    def forward_early_status(self, g: GaussianTensors, cam: Camera, out_color: torch.Tensor,
+                             radii: torch.Tensor, D: int = 3, scale_modifier: float = 1.0,
+                             stream=None) -> tuple[int, int]:
+        """Forward that returns (num_rendered, status bits) once the binning has run; the blend
+        is still executing on ``stream`` when it returns."""
+        assert (cam.width, cam.height) == (self.W, self.H) and g.P == self.P
+        a = self._fwd_args(g, cam, out_color, radii, D, scale_modifier)
+        n = ctypes.c_int(0)
+        st = ctypes.c_uint32(0)
+        rc = capi.lib().omnigs_lonlat_forward_early_status(
+            ctypes.byref(a), self.geom.data_ptr(), self.geom.numel(), self.binning.data_ptr(),
+            self.binning.numel(), self.image.data_ptr(), self.image.numel(), ctypes.byref(n),
+            ctypes.byref(st), capi.stream_handle(stream))
+        capi.check(rc, "omnigs_lonlat_forward_early_status")
+        return int(n.value), int(st.value)
+
     def render(self, g: GaussianTensors, cam: Camera, out_color, radii, D=3, scale_modifier=1.0,
                stream=None):
         """Re-run binning + blend from the current geometry buffer (after a capacity resize)."""

@@ -172,6 +172,41 @@ def test_capacity_overflow_is_reported_and_resumable(cuda):
     torch.testing.assert_close(out, full["image"], rtol=0, atol=0)
 
 
+def test_forward_early_status_matches_forward_and_read_status(cuda):
+    """The forward that returns num_rendered and the status once the binning has run gives the same
+    image, radii, per-pixel state, count and status as forward + read_status, also when the
+    binning capacity is too small (then the count is the required capacity)."""
+    W, H = 1024, 512
+    g, v, gt, cam = _scene(40_000, W, H, seed=21)
+    runs = {}
+    for mode in ("read_status", "early"):
+        state = lonlat.LonlatState(g.P, W, H, capacity=2_000_000)
+        out = torch.empty(3, H, W, device="cuda")
+        radii = torch.empty(g.P, dtype=torch.int32, device="cuda")
+        for _ in range(2):  # the second call reuses the thread's pinned status slot
+            if mode == "early":
+                n, st = state.forward_early_status(gt, cam, out, radii)
+            else:
+                state.forward(gt, cam, out, radii)
+                n, st = state.status()
+        torch.cuda.synchronize()
+        iv = state.image_view()
+        runs[mode] = (n, st, out.clone(), radii.clone(), iv["final_T"].clone(), iv["n_contrib"].clone())
+    a, b = runs["read_status"], runs["early"]
+    assert a[0] == b[0] and a[0] > 0 and a[1] == b[1] == 0
+    for x, y in zip(a[2:], b[2:]):
+        assert torch.equal(x, y)
+    small = lonlat.LonlatState(g.P, W, H, capacity=100)
+    out = torch.empty(3, H, W, device="cuda")
+    radii = torch.empty(g.P, dtype=torch.int32, device="cuda")
+    n, st = small.forward_early_status(gt, cam, out, radii)
+    assert st & 1 and n == a[0]
+    small.resize_capacity(n)
+    small.render(gt, cam, out, radii)
+    assert small.status() == (a[0], 0)
+    assert torch.equal(out, a[2])
+
+
 def test_repeated_backward_is_consistent(cuda):
     W, H = 256, 128
     g, v, gt, cam = _scene(3000, W, H, seed=9)
