@@ -53,6 +53,41 @@ __device__ __forceinline__ void load_sh(const void* shs, int g, int M, float out
   }
 }
 
+// Warp-cooperative staging of FP32 SH (M == 16): the warp's 32 consecutive Gaussians own one
+// contiguous 6 KB span, which the warp loads with 12 fully coalesced 16-byte loads per lane (each
+// instruction reads 512 contiguous bytes) into `stage`, instead of each lane reading its own 192 B
+// (every warp instruction then touches 32 separate cache lines).  `stage` holds kShStageStride
+// float4 per Gaussian: the spare float4 puts the 16-byte reads of 8 lanes (one shared-memory
+// phase) of their own records on distinct banks.  warp_stage_sh is warp-uniform; it returns false,
+// loading nothing, unless the whole warp qualifies (full warp, M == 16, 16-byte aligned).
+constexpr int kShStageStride = 13;
+
+__device__ __forceinline__ bool warp_stage_sh(const float* shs, int first, int P, int M, float4* stage, int lane) {
+  if (shs == nullptr || M != kMaxShCoeffs || first + 32 > P || (reinterpret_cast<uintptr_t>(shs) & 15) != 0)
+    return false;
+  const float4* src = reinterpret_cast<const float4*>(shs) + (size_t)first * 12;
+#pragma unroll
+  for (int i = 0; i < 12; ++i) {
+    const int e = i * 32 + lane;
+    const int gg = e / 12, part = e - gg * 12;
+    stage[gg * kShStageStride + part] = __ldg(src + e);
+  }
+  __syncwarp();
+  return true;
+}
+
+// This lane's 48 staged coefficients.
+__device__ __forceinline__ void read_staged_sh(const float4* stage, int lane, float out[3 * kMaxShCoeffs]) {
+#pragma unroll
+  for (int i = 0; i < 12; ++i) {
+    const float4 f = stage[lane * kShStageStride + i];
+    out[4 * i] = f.x;
+    out[4 * i + 1] = f.y;
+    out[4 * i + 2] = f.z;
+    out[4 * i + 3] = f.w;
+  }
+}
+
 // Writes the gradient of Gaussian g's M coefficients at d (= dL_dsh + g M 3): v[3k + ch] for
 // k < ncoef, zeros for the remaining coefficients.
 __device__ __forceinline__ void store_sh_grad(float* d, int M, int ncoef, const float v[3 * kMaxShCoeffs]) {
