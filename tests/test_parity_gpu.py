@@ -208,6 +208,10 @@ def test_forward_early_status_matches_forward_and_read_status(cuda):
 
 
 def test_repeated_backward_is_consistent(cuda):
+    """A second backward on the same state gives the same gradients (the accumulator records are
+    consumed and cleared, nothing leaks between calls).  The blend adds its per-splat sums with
+    float atomics whose order varies between runs, so the comparison is normwise (max |a - b| over
+    max |b|, per tensor) at 1e-5; a leaked accumulation would show as an error of order 1."""
     W, H = 256, 128
     g, v, gt, cam = _scene(3000, W, H, seed=9)
     img, radii, n, state = lonlat.rasterize(gt, cam)
@@ -217,7 +221,8 @@ def test_repeated_backward_is_consistent(cuda):
     state.backward(gt, cam, radii, dpix, g1, R=n)
     state.backward(gt, cam, radii, dpix, g2, R=n)
     for name in ("dL_dmeans3D", "dL_dsh", "dL_dopacity", "dL_dmeans2D"):
-        torch.testing.assert_close(getattr(g1, name), getattr(g2, name), rtol=1e-5, atol=1e-6)
+        a, b = getattr(g1, name).double(), getattr(g2, name).double()
+        assert float((a - b).abs().max()) <= 1e-5 * float(b.abs().max()), name
 
 
 def test_full_size_properties(cuda):
