@@ -114,7 +114,7 @@ __global__ void mark_visible_kernel(int P, const float* means3D, const float* vm
 
 void set_last_error(const char* msg) { g_last_error = msg; }
 
-std::atomic<int> g_blend_batch[2] = {{kDefaultBatch}, {kDefaultBatch}};
+std::atomic<int> g_blend_batch[2] = {{kDefaultBatch}, {kDefaultBwdBatch}};
 int blend_batch_size(bool backward) { return g_blend_batch[backward ? 1 : 0].load(std::memory_order_relaxed); }
 
 void launch_mark_visible(int P, const float* means3D, const float* viewmatrix, int camera_type,
