@@ -18,7 +18,10 @@ across ranks every step with one NCCL all-reduce, as a data-parallel train step 
   loop would pipeline them.  The Gaussian parameters and their gradients stay on the device, as in
   the reference trainer.
 * roofline: per-kernel device times from the library's event timing, against the algorithmic bytes
-  of each stage; the dominant kernel is reported against MEASURED_PEAKS.json.
+  of each stage; the dominant kernel is reported against MEASURED_PEAKS.json.  roofline_fp32 puts
+  the blends against the FP32 issue peak (they are FP32/MUFU-issue-bound, not HBM-bound), and
+  path_roofline sums every stage's lower-bound time (bytes at the HBM peak or FP32 work at the FP32
+  peak) over the measured step time.
 * cpu_baseline: the FP64 oracle (multithreaded C++ restatement of the reference algorithm) on the
   same view, on this host's cores.
 * --impl reference: the reference arm.  The reference's rasterizer is CUDA-only, so its CPU
@@ -611,6 +614,17 @@ def run_omnigs(args, rank, world, local_rank):
                      "flops_per_pair": 24 if k == "render_forward" else 64}
     roofline_fp32 = {"bound": "fp32", "peak_tflops": round(fp32_peak, 1),
                      "peak_source": "nominal 148 SM x 128 FP32 lanes x 2 x sm_max_mhz", **rf}
+    # whole-path roofline: each stage's lower-bound time (its algorithmic bytes at the HBM peak, or
+    # for the blends its FP32 work at the FP32 peak, whichever is longer) summed over the stages,
+    # over the measured step time
+    stage_flops = {"render_forward": flops_fwd, "render_backward": flops_bwd}
+    bound_ms = {k: max(sbytes[k] / (hbm_peak * 1e9), stage_flops.get(k, 0) / (fp32_peak * 1e12)) * 1e3
+                for k in kernels}
+    path_roofline = {"frac": round(sum(bound_ms.values()) / ms_per_step, 4),
+                     "bound_ms_per_step": round(sum(bound_ms.values()), 4), "measured_ms_per_step": round(ms_per_step, 4),
+                     "stage_bound_ms": {k: round(v, 4) for k, v in bound_ms.items()},
+                     "formula": "sum over stages of max(algorithmic bytes / HBM peak, FP32 flops / FP32 peak), "
+                                "over the measured fwd+bwd step time"}
 
     # ---- end to end through the reference-facing LibTorch API with host buffers ----
     e2e = None
@@ -710,8 +724,8 @@ def run_omnigs(args, rank, world, local_rank):
                            "num_rendered": n0, "visible": V, "parallelism": f"dp{world} (views)",
                            "l2": "inputs larger than L2 (SH alone 192 MB > 126 MB), no flush"},
                 "gpu_launches": int(launches), "clocks": clocks.summary(), "roofline": roofline,
-                "roofline_fp32": roofline_fp32, "kernels": kernels, "e2e": e2e, "batched": batched, "configs": extra,
-                "cpu_baseline": cpu}
+                "roofline_fp32": roofline_fp32, "path_roofline": path_roofline, "kernels": kernels, "e2e": e2e,
+                "batched": batched, "configs": extra, "cpu_baseline": cpu}
         print(json.dumps(line), flush=True)
 
 
