@@ -738,8 +738,12 @@ def main():
     if world > 1:
         import datetime
 
+        import torch
         import torch.distributed as dist
-        dist.init_process_group("nccl", timeout=datetime.timedelta(seconds=120))
+        # bind this rank's GPU before NCCL sets up its communicator
+        torch.cuda.set_device(local_rank)
+        dist.init_process_group("nccl", timeout=datetime.timedelta(seconds=120),
+                                device_id=torch.device("cuda", local_rank))
     try:
         run_omnigs(args, rank, world, local_rank)
     finally:
