@@ -71,6 +71,20 @@ def test_forward_argument_validation_precedes_device_work(over, code):
     assert capi.lib().omnigs_last_error()
 
 
+@pytest.mark.parametrize("over,code", [(dict(P=-1), 1), (dict(D=4), 1), (dict(radii=None), 1)])
+def test_forward_early_status_validates_before_device_work(over, code):
+    a = _fake_args(**over)
+    n, st = ctypes.c_int(-1), ctypes.c_uint32(7)
+    rc = capi.lib().omnigs_lonlat_forward_early_status(ctypes.byref(a), 0x10000, 1 << 30, 0x10000, 1 << 30,
+                                                       0x10000, 1 << 30, ctypes.byref(n), ctypes.byref(st), None)
+    assert rc == code and capi.lib().omnigs_last_error()
+    # the two host outputs are required
+    a = _fake_args()
+    rc = capi.lib().omnigs_lonlat_forward_early_status(ctypes.byref(a), 0x10000, 1 << 30, 0x10000, 1 << 30,
+                                                       0x10000, 1 << 30, None, ctypes.byref(st), None)
+    assert rc == 1 and b"num_rendered" in capi.lib().omnigs_last_error()
+
+
 def test_forward_rejects_small_buffers():
     a = _fake_args()
     rc = capi.lib().omnigs_lonlat_preprocess(ctypes.byref(a), 0x10000, 16, None)
