@@ -307,6 +307,7 @@ __global__ void __launch_bounds__(kScanBlock) duplicate_kernel(const __grid_cons
   const uint32_t i = tile * kScanBlock + threadIdx.x;
   uint32_t count = 0, g = 0, row_origin = 0;
   int pitch = 1, width = 1, col0 = 0;
+  float inv_width = 1.f;
   if (i < items) {
     const uint32_t view = (p.V == 1) ? 0u : i / (uint32_t)p.P;  // the order keeps records in their view
     g = p.order[i];
@@ -322,6 +323,7 @@ __global__ void __launch_bounds__(kScanBlock) duplicate_kernel(const __grid_cons
       width = rmax.x - rmin.x;
       count = (uint32_t)width * (uint32_t)(rmax.y - rmin.y);
       if (count == 0) width = 1;
+      inv_width = 1.f / (float)width;
       pitch = gx;
       col0 = rmin.x;
       row_origin = p.tile_base[view] + (uint32_t)rmin.y * (uint32_t)gx;
@@ -414,14 +416,25 @@ __global__ void __launch_bounds__(kScanBlock) duplicate_kernel(const __grid_cons
     const uint32_t o_origin = __shfl_sync(kFullMask, row_origin, pos);
     const int o_pitch = __shfl_sync(kFullMask, pitch, pos);
     const int o_width = __shfl_sync(kFullMask, width, pos);
+    const float o_inv = __shfl_sync(kFullMask, inv_width, pos);
     const int o_col0 = __shfl_sync(kFullMask, col0, pos);
     const uint32_t o_g = __shfl_sync(kFullMask, g, pos);
     const bool ok = o < w_end && o < limit;
     uint32_t key = 0;
     if (ok) {
       const uint32_t local = o - o_start;
-      const uint32_t ry = local / (uint32_t)o_width;
-      int tx = o_col0 + (int)(local - ry * (uint32_t)o_width);
+      // local / width from the float reciprocal: local < 2^21 (a rect holds at most every tile of
+      // a view), so the truncated estimate is within one of the quotient; one step fixes it
+      uint32_t ry = (uint32_t)((float)local * o_inv);
+      int rem = (int)(local - ry * (uint32_t)o_width);
+      if (rem < 0) {
+        ry -= 1u;
+        rem += o_width;
+      } else if (rem >= o_width) {
+        ry += 1u;
+        rem -= o_width;
+      }
+      int tx = o_col0 + rem;
       if (tx < 0) tx += o_pitch;  // seam wrap: columns left of 0 or right of gx - 1
       if (tx >= o_pitch) tx -= o_pitch;
       key = o_origin + ry * (uint32_t)o_pitch + (uint32_t)tx;
