@@ -23,8 +23,29 @@ struct BatchPlan {
   int64_t pixels = 0, tiles = 0;
   int64_t pixel_base[kMaxBatchViews] = {};
   int64_t tile_base[kMaxBatchViews] = {};
+  int64_t view_tiles[kMaxBatchViews] = {};
   uint8_t tile_order[kMaxBatchViews] = {};
+  int P = 0;
 };
+
+// The tile sort of a batch.  Each view's instances leave the duplicate pass contiguous (view after
+// view), so the sort can run per view on view-local tile ids, which need fewer digits than the
+// batch's global ids when the views together hold more than 2^k tiles and the largest alone fewer.
+// Per view, each segment has its own digit histograms (counted by the duplicate pass, which needs
+// P >= kScanBlock so that one of its blocks spans at most two views) and its own look-back chain.
+struct BatchTileSort {
+  TileDigits digits;
+  bool per_view;
+};
+
+BatchTileSort batch_tile_sort(const BatchPlan& plan) {
+  const TileDigits global = TileDigits::from_tiles((uint32_t)plan.tiles);
+  int64_t max_view_tiles = 1;
+  for (int v = 0; v < plan.V; ++v) max_view_tiles = std::max(max_view_tiles, plan.view_tiles[v]);
+  const TileDigits local = TileDigits::from_tiles((uint32_t)max_view_tiles);
+  const bool per_view = plan.V > 1 && plan.P >= kScanBlock && local.passes < global.passes;
+  return {per_view ? local : global, per_view};
+}
 
 int make_plan(int P, int V, const int* W, const int* H, BatchPlan& plan) {
   if (P < 0) return fail(OMNIGS_ERR_INVALID_ARGUMENT, "P must be >= 0");
@@ -34,6 +55,7 @@ int make_plan(int P, int V, const int* W, const int* H, BatchPlan& plan) {
   if ((int64_t)P * V > (int64_t(1) << 31))
     return fail(OMNIGS_ERR_INVALID_ARGUMENT, "P * V must be at most 2^31 (records are indexed by 32 bits)");
   plan.V = V;
+  plan.P = P;
   int64_t order[kMaxBatchViews];
   for (int v = 0; v < V; ++v) {
     if (W[v] <= 0 || H[v] <= 0 || W[v] > 65536 || H[v] > 65536 || (int64_t)W[v] * H[v] > (int64_t(1) << 28))
@@ -50,7 +72,8 @@ int make_plan(int P, int V, const int* W, const int* H, BatchPlan& plan) {
     const int v = (int)order[k];
     plan.tile_order[k] = (uint8_t)v;
     plan.tile_base[v] = plan.tiles;
-    plan.tiles += (int64_t)tiles_x(W[v]) * tiles_y(H[v]);
+    plan.view_tiles[v] = (int64_t)tiles_x(W[v]) * tiles_y(H[v]);
+    plan.tiles += plan.view_tiles[v];
   }
   if (plan.pixels > 0xffffffffll)
     return fail(OMNIGS_ERR_INVALID_ARGUMENT, "a batch holds at most 2^32 - 1 pixels");
@@ -195,7 +218,6 @@ int omnigs_batch_render(const OmnigsBatchArgs* a, void* state, size_t state_byte
     return fail(OMNIGS_ERR_BUFFER_TOO_SMALL, "binning buffer smaller than omnigs_lonlat_binning_bytes(0)");
   const BinningLayout BL = BinningLayout::make(capacity);
   if (capacity > kMaxInstances) capacity = kMaxInstances;
-  const TileDigits td = TileDigits::from_tiles((uint32_t)plan.tiles);
   const BatchParams bp = batch_params(a, plan, state, L);
   GeomHeader* hdr = bp.hdr;
   uint32_t* thist = at<uint32_t>(binning, BL.hist);
@@ -206,8 +228,6 @@ int omnigs_batch_render(const OmnigsBatchArgs* a, void* state, size_t state_byte
   staged(OMNIGS_STAGE_OTHER, 1, s, [&] { launch_begin_render(hdr, s); });
   if (cudaMemsetAsync(at<unsigned char>(state, L.dup_scan), 0, L.zero_end - L.dup_scan, s) != cudaSuccess ||
       cudaMemsetAsync(thist, 0, sizeof(uint32_t) * kMaxSortPasses * kRadix, s) != cudaSuccess ||
-      cudaMemsetAsync(at<uint32_t>(binning, BL.tile_lookback), 0, sizeof(uint32_t) * td.passes * inst_tiles * kRadix,
-                      s) != cudaSuccess ||
       cudaMemsetAsync(at<uint2>(state, L.ranges), 0, sizeof(uint2) * plan.tiles, s) != cudaSuccess)
     return check_launch("memset batch binning state");
 
@@ -268,33 +288,50 @@ int omnigs_batch_render(const OmnigsBatchArgs* a, void* state, size_t state_byte
     d.gy[v] = bp.views[v].gy;
     d.tile_base[v] = bp.views[v].tile_base;
   }
-  d.hist = thist + kDepthPasses * kRadix;
-  d.hist_passes = td.passes;
-  for (int q = 0; q < td.passes; ++q) {
-    d.hist_shift[q] = td.shift[q];
-    d.hist_mask[q] = td.mask[q];
+  // tile sort per view or over the global tile ids (batch_tile_sort)
+  const BatchTileSort ts = batch_tile_sort(plan);
+  const bool per_view = ts.per_view;
+  const TileDigits& tds = ts.digits;
+  uint32_t* tile_hist = per_view ? at<uint32_t>(state, L.tile_hist) : thist + kDepthPasses * kRadix;
+  const int64_t lb_tiles = inst_tiles + a->V;  // look-back tiles per pass (per view: partial tiles)
+  if (cudaMemsetAsync(at<uint32_t>(binning, BL.tile_lookback), 0, sizeof(uint32_t) * tds.passes * lb_tiles * kRadix,
+                      s) != cudaSuccess)
+    return check_launch("memset tile look-back");
+  d.hist = tile_hist;
+  d.hist_passes = tds.passes;
+  d.hist_per_view = per_view ? 1 : 0;
+  d.key_base_out = at<uint32_t>(state, L.view_key_base);
+  for (int q = 0; q < tds.passes; ++q) {
+    d.hist_shift[q] = tds.shift[q];
+    d.hist_mask[q] = tds.mask[q];
   }
   staged(OMNIGS_STAGE_DUPLICATE, 1, s, [&] { launch_duplicate(d, s); });
 
-  // 3. stable tile sort of all instances
-  // (its digit histograms were counted by the duplicate pass)
-  for (int q = 0; q < td.passes; ++q) {
+  // 3. stable tile sort of all instances (per view when per_view; the digit histograms were
+  // counted by the duplicate pass)
+  for (int q = 0; q < tds.passes; ++q) {
     OnesweepParams op{};
     op.keys_in = tkeys[q & 1];
     op.vals_in = tvals[q & 1];
     op.keys_out = tkeys[(q + 1) & 1];
     op.vals_out = tvals[(q + 1) & 1];
-    op.shift = td.shift[q];
-    op.mask = td.mask[q];
+    op.shift = tds.shift[q];
+    op.mask = tds.mask[q];
     op.count_hdr = hdr;
     op.capacity = capacity;
-    op.hist = thist + (kDepthPasses + q) * kRadix;
-    op.lookback = at<uint32_t>(binning, BL.tile_lookback) + (size_t)q * inst_tiles * kRadix;
+    op.hist = tile_hist + q * kRadix;
+    op.lookback = at<uint32_t>(binning, BL.tile_lookback) + (size_t)q * lb_tiles * kRadix;
     op.tile_counter = &hdr->sort_tile_counter[kDepthPasses + q];
     op.hdr = hdr;
+    if (per_view) {
+      op.seg_counts = bp.view_rendered;
+      op.num_segs = (uint32_t)a->V;
+      op.hist_seg_stride = kTilePasses * kRadix;
+      op.add_key_base = q == tds.passes - 1;
+    }
     staged(OMNIGS_STAGE_SORT, 1, s, [&] { launch_onesweep(op, capacity, s); });
   }
-  const int fin = td.passes & 1;
+  const int fin = tds.passes & 1;
   if (int rc = check_launch("batch binning")) return rc;
 
   // 4. tile ranges over all views' tiles
@@ -350,7 +387,7 @@ int omnigs_batch_backward(const OmnigsBatchArgs* a, const OmnigsBatchGrads* g, v
     return fail(OMNIGS_ERR_BUFFER_TOO_SMALL, "binning buffer smaller than omnigs_lonlat_binning_bytes(0)");
   const BinningLayout BL = BinningLayout::make(capacity);
   if (capacity > kMaxInstances) capacity = kMaxInstances;
-  const int fin = TileDigits::from_tiles((uint32_t)plan.tiles).passes & 1;
+  const int fin = batch_tile_sort(plan).digits.passes & 1;
   cudaStream_t s = reinterpret_cast<cudaStream_t>(stream);
   const BatchParams bp = batch_params(a, plan, state, L);
   const BatchRenderParams r =
@@ -402,7 +439,7 @@ int omnigs_batch_autotune(const OmnigsBatchArgs* a, void* state, size_t state_by
     return check_launch("read batch status");
   if (h.status != 0)
     return fail(OMNIGS_ERR_DEVICE, "the batch state holds no complete forward (status word set); run omnigs_batch_forward first");
-  const int fin = TileDigits::from_tiles((uint32_t)plan.tiles).passes & 1;
+  const int fin = batch_tile_sort(plan).digits.passes & 1;
   const BatchParams bp = batch_params(a, plan, state, L);
   const BatchRenderParams r =
       render_params(bp, plan, state, L, at<uint32_t>(binning, fin ? BL.tvals1 : BL.tvals0), capacity);
@@ -490,7 +527,7 @@ int omnigs_batch_state_view(const void* state, int P, int V, const int* W, const
     out->pixel_base[v] = plan.pixel_base[v];
     out->tile_base[v] = plan.tile_base[v];
   }
-  out->tile_passes = TileDigits::from_tiles((uint32_t)plan.tiles).passes;
+  out->tile_passes = batch_tile_sort(plan).digits.passes;
   return OMNIGS_OK;
 }
 

@@ -109,6 +109,9 @@ struct SortSmem {
   uint32_t pad[3];
   uint32_t keys[kSortTile];
   uint32_t vals[kSortTile];
+  // the block's segment as thread 0 resolved it (variable segments): index (num_segs: none), item
+  // count, tile within the segment, first item, key base
+  uint32_t seg, seg_n, seg_tile, seg_first, seg_key_base;
 };
 
 // Exclusive scan of one value per thread across the block (kSortThreads == kRadix == 256).
@@ -144,20 +147,63 @@ __device__ __forceinline__ uint32_t block_exclusive_scan(uint32_t v, uint32_t* s
 // decoupled look-back (tiles are taken in launch order from an atomic counter, so a block only
 // waits on blocks that are already running) and writes runs of equal digits coalesced.  In a
 // segmented sort every segment is an independent sort whose look-back chain starts at the
-// segment's first tile; a value-less first pass numbers items by their global index.
+// segment's first tile (segments of equal length, or of device-side lengths, whose keys are then
+// segment-local and get seg_key_base added back in the last pass); a value-less first pass numbers
+// items by their global index.
+// Launches of this pass measured ~2 us slower each on a B200 with a 136-byte parameter block than
+// with a 128-byte one.
+static_assert(sizeof(OnesweepParams) <= 128, "keep the onesweep parameter block at 128 bytes or less");
+
+template <bool kVarSeg>
 __global__ void __launch_bounds__(kSortThreads, 3) onesweep_kernel(OnesweepParams p) {
   __shared__ SortSmem sm;
-  const uint32_t n = p.seg_len ? p.seg_len : item_count(p.count_hdr, p.n_host, p.capacity);
-  const uint32_t tiles_per_seg = (n + kSortTile - 1) / kSortTile;
-  const uint32_t ntiles = tiles_per_seg * (p.seg_len ? p.num_segs : 1u);
-  if (threadIdx.x == 0) sm.tile = atomicAdd(p.tile_counter, 1u);
+  uint32_t n = 0, tiles_per_seg = 1, ntiles = 0;
+  if (!kVarSeg) {
+    n = p.seg_len ? p.seg_len : item_count(p.count_hdr, p.n_host, p.capacity);
+    tiles_per_seg = (n + kSortTile - 1) / kSortTile;
+    ntiles = tiles_per_seg * (p.seg_len ? p.num_segs : 1u);
+  }
+  if (threadIdx.x == 0) {
+    const uint32_t t = atomicAdd(p.tile_counter, 1u);
+    sm.tile = t;
+    if (kVarSeg) {  // variable segments: tickets run over the segments' tiles in order
+      const bool fit = instances_fit(p.count_hdr, p.capacity);
+      uint32_t first_tile = 0, first_item = 0;
+      sm.seg = p.num_segs;
+      for (uint32_t sg = 0; sg < p.num_segs; ++sg) {
+        const uint32_t ns = fit ? (uint32_t)p.seg_counts[sg] : 0u;
+        const uint32_t ts = (ns + kSortTile - 1) / kSortTile;
+        if (t < first_tile + ts) {
+          sm.seg = sg;
+          sm.seg_n = ns;
+          sm.seg_tile = t - first_tile;
+          sm.seg_first = first_item;
+          sm.seg_key_base = reinterpret_cast<const uint32_t*>(p.seg_counts + kMaxBatchViews)[sg];
+          break;
+        }
+        first_tile += ts;
+        first_item += ns;
+      }
+    }
+  }
   for (int i = threadIdx.x; i < (kSortThreads / 32) * kRadix; i += kSortThreads) (&sm.warp_hist[0][0])[i] = 0;
   __syncthreads();
   const uint32_t ticket = sm.tile;
-  if (ticket >= ntiles) return;
-  const uint32_t seg = ticket / tiles_per_seg;
-  const uint32_t tile = ticket - seg * tiles_per_seg;  // tile index within the segment
-  const size_t seg_base = (size_t)seg * n;
+  // this block's segment, its item count and first item, and the tile index within it
+  uint32_t seg, tile;
+  size_t seg_base;
+  if (kVarSeg) {
+    seg = sm.seg;
+    if (seg >= p.num_segs) return;
+    n = sm.seg_n;
+    tile = sm.seg_tile;
+    seg_base = sm.seg_first;
+  } else {
+    if (ticket >= ntiles) return;
+    seg = ticket / tiles_per_seg;
+    tile = ticket - seg * tiles_per_seg;  // tile index within the segment
+    seg_base = (size_t)seg * n;
+  }
   const uint32_t* keys_in = p.keys_in + seg_base;
   const uint32_t* vals_in = p.vals_in ? p.vals_in + seg_base : nullptr;
   uint32_t* keys_out = p.keys_out + seg_base;
@@ -271,12 +317,14 @@ __global__ void __launch_bounds__(kSortThreads, 3) onesweep_kernel(OnesweepParam
     }
   }
   __syncthreads();
+  // the last pass of a variable-segment sort turns segment-local keys back into global ones
+  const uint32_t key_add = (kVarSeg && p.add_key_base) ? sm.seg_key_base : 0u;
   for (uint32_t i = threadIdx.x; i < tile_items; i += kSortThreads) {
     const uint32_t k32 = sm.keys[i];
     const uint32_t digit = (k32 >> shift) & mask;
     const uint32_t out = sm.global_base[digit] + (i - sm.block_excl[digit]);
     if (out < n) {  // always true unless a look-back gave up (the status word then says so)
-      keys_out[out] = k32;
+      keys_out[out] = k32 + key_add;
       vals_out[out] = sm.vals[i];
     }
   }
@@ -289,27 +337,35 @@ __global__ void __launch_bounds__(kSortThreads, 3) onesweep_kernel(OnesweepParam
 // plus a decoupled look-back over the preceding blocks.  Each warp then writes the instances of
 // its 32 Gaussians (one contiguous span) 32 at a time: a 5-step shuffle search finds each
 // instance's Gaussian, so a splat covering hundreds of tiles does not serialise one thread.
+template <bool kPerView>
 __global__ void __launch_bounds__(kScanBlock) duplicate_kernel(const __grid_constant__ DuplicateParams p) {
   __shared__ uint32_t s_tile;
   __shared__ uint32_t s_warp[kScanBlock / 32];
   __shared__ unsigned long long s_excl;
-  __shared__ uint32_t s_hist[kTilePasses][kRadix];
+  // digit counts of the tile sort: [slot][pass][digit], slot = view - (the block's first view)
+  // when counted per view (a block then spans at most two views), else one slot
+  constexpr int kHistSlot = kTilePasses * kRadix;
+  constexpr int kSlots = kPerView ? 2 : 1;
+  __shared__ uint32_t s_hist[kSlots * kHistSlot];
   if (!instances_fit(p.hdr, p.capacity)) {
     if (blockIdx.x == 0 && threadIdx.x == 0) atomicOr(&p.hdr->status, kStatusCapacity);
     return;
   }
+  if (kPerView && blockIdx.x == 0 && threadIdx.x < p.V) p.key_base_out[threadIdx.x] = p.tile_base[threadIdx.x];
   if (threadIdx.x == 0) s_tile = atomicAdd(&p.hdr->dup_tile_counter, 1u);
-  for (int k = threadIdx.x; k < kTilePasses * kRadix; k += kScanBlock) (&s_hist[0][0])[k] = 0;
+  for (int k = threadIdx.x; k < kSlots * kHistSlot; k += kScanBlock) s_hist[k] = 0;
   __syncthreads();
   const uint32_t tile = s_tile;
   const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
   const uint32_t items = (uint32_t)p.P * (uint32_t)p.V;
   const uint32_t i = tile * kScanBlock + threadIdx.x;
-  uint32_t count = 0, g = 0, row_origin = 0;
+  const uint32_t view0 = (p.V == 1) ? 0u : (tile * kScanBlock) / (uint32_t)p.P;
+  uint32_t count = 0, g = 0, row_origin = 0, my_view = view0;
   int pitch = 1, width = 1, col0 = 0;
   float inv_width = 1.f;
   if (i < items) {
     const uint32_t view = (p.V == 1) ? 0u : i / (uint32_t)p.P;  // the order keeps records in their view
+    my_view = view;
     g = p.order[i];
     const int radius = (g - view * (uint32_t)p.P < (uint32_t)p.P) ? p.radii[g] : 0;
     if (radius > 0) {
@@ -326,7 +382,8 @@ __global__ void __launch_bounds__(kScanBlock) duplicate_kernel(const __grid_cons
       inv_width = 1.f / (float)width;
       pitch = gx;
       col0 = rmin.x;
-      row_origin = p.tile_base[view] + (uint32_t)rmin.y * (uint32_t)gx;
+      // per-view counting writes view-local tile ids (the tile sort restores the global ids)
+      row_origin = (kPerView ? 0u : p.tile_base[view]) + (uint32_t)rmin.y * (uint32_t)gx;
     }
   }
   // block inclusive scan of the counts
@@ -443,15 +500,22 @@ __global__ void __launch_bounds__(kScanBlock) duplicate_kernel(const __grid_cons
     }
     // digit histograms of the tile sort (the pass that would otherwise re-read every key)
     const unsigned live = __ballot_sync(kFullMask, ok);
+    const uint32_t slot = kPerView ? __shfl_sync(kFullMask, my_view, pos) - view0 : 0u;
 #pragma unroll
     for (int q = 0; q < kTilePasses; ++q)
-      if (q < p.hist_passes) count_digit(s_hist[q], (key >> p.hist_shift[q]) & p.hist_mask[q], ok, live, lane);
+      if (q < p.hist_passes)
+        count_digit(s_hist, slot * kHistSlot + q * kRadix + ((key >> p.hist_shift[q]) & p.hist_mask[q]), ok, live,
+                    lane);
   }
   if (p.hist_passes == 0) return;
   __syncthreads();
-  for (int k = threadIdx.x; k < p.hist_passes * kRadix; k += kScanBlock) {
-    const uint32_t c = (&s_hist[0][0])[k];
-    if (c) atomicAdd(&p.hist[k], c);
+  for (int k = threadIdx.x; k < kSlots * kHistSlot; k += kScanBlock) {
+    const uint32_t c = s_hist[k];
+    if (c == 0) continue;
+    if (kPerView)
+      atomicAdd(&p.hist[(size_t)(view0 + (uint32_t)(k / kHistSlot)) * kHistSlot + (k % kHistSlot)], c);
+    else
+      atomicAdd(&p.hist[k], c);
   }
 }
 
@@ -493,15 +557,25 @@ void launch_histogram(const HistParams& p, int64_t max_items, cudaStream_t s) {
 }
 
 void launch_onesweep(const OnesweepParams& p, int64_t max_items, cudaStream_t s) {
-  const int64_t blocks = p.seg_len ? sort_tiles(p.seg_len) * (int64_t)p.num_segs : sort_tiles(max_items);
+  // variable segments: each segment's last tile may be partial, so up to num_segs extra tiles
+  const int64_t blocks = p.seg_counts ? sort_tiles(max_items) + (int64_t)p.num_segs
+                         : p.seg_len  ? sort_tiles(p.seg_len) * (int64_t)p.num_segs
+                                      : sort_tiles(max_items);
   if (blocks <= 0) return;
-  onesweep_kernel<<<(unsigned)blocks, kSortThreads, 0, s>>>(p);
+  if (p.seg_counts)
+    onesweep_kernel<true><<<(unsigned)blocks, kSortThreads, 0, s>>>(p);
+  else
+    onesweep_kernel<false><<<(unsigned)blocks, kSortThreads, 0, s>>>(p);
 }
 
 void launch_duplicate(const DuplicateParams& p, cudaStream_t s) {
   const int64_t items = (int64_t)p.P * p.V;
   if (items <= 0) return;
-  duplicate_kernel<<<(unsigned)((items + kScanBlock - 1) / kScanBlock), kScanBlock, 0, s>>>(p);
+  const unsigned blocks = (unsigned)((items + kScanBlock - 1) / kScanBlock);
+  if (p.hist_per_view)
+    duplicate_kernel<true><<<blocks, kScanBlock, 0, s>>>(p);
+  else
+    duplicate_kernel<false><<<blocks, kScanBlock, 0, s>>>(p);
 }
 
 void launch_ranges(const RangesParams& p, cudaStream_t s) {

@@ -8,8 +8,6 @@
 
 namespace omnigs {
 
-// Views per batched launch.
-constexpr int kMaxBatchViews = 32;
 
 struct PreprocessParams {
   int P, D, M, W, H, gx, gy;
@@ -68,6 +66,14 @@ struct OnesweepParams {
   uint32_t seg_len;
   uint32_t num_segs;
   uint32_t hist_seg_stride;
+  // Variable segments (seg_counts non-null): num_segs consecutive segments of seg_counts[s] items
+  // (device counts, all taken as 0 when count_hdr reports an overflow) with segment-local keys;
+  // with add_key_base the pass writes key + (segment s's key base) (the last pass restores global
+  // keys).  The key bases are the u32[kMaxBatchViews] array that directly follows the
+  // u64[kMaxBatchViews] counts (BatchLayout), so this parameter block stays at 128 bytes: at 136
+  // bytes every launch of the pass measured ~2 us slower on a B200.
+  const unsigned long long* seg_counts;
+  int add_key_base;
 };
 
 // duplicateWithKeys over V views (V = 1 for a single view).  Records are view-major (rec = v P + g);
@@ -86,11 +92,15 @@ struct DuplicateParams {
   int gx[kMaxBatchViews], gy[kMaxBatchViews];
   uint32_t tile_base[kMaxBatchViews];
   // digit histograms of the tile sort, accumulated into hist[hist_passes][kRadix] (zeroed by the
-  // caller); hist_passes 0 counts nothing
+  // caller); hist_passes 0 counts nothing.  With hist_per_view, the keys written are view-local
+  // tile ids (without tile_base[v]) and each view's digits are counted into
+  // hist + v * kTilePasses * kRadix (requires P >= kScanBlock: a block then spans at most two views).
   uint32_t* hist;
   int hist_passes;
   int hist_shift[kTilePasses];
   uint32_t hist_mask[kTilePasses];
+  int hist_per_view;
+  uint32_t* key_base_out;      // with hist_per_view: tile_base[0, V) copied here for the tile sort
 };
 
 struct RangesParams {

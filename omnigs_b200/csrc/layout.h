@@ -31,6 +31,7 @@
 namespace omnigs {
 
 constexpr size_t kAlign = 256;
+constexpr int kMaxBatchViews = 32;           // views per batched launch
 constexpr int kScanBlock = 256;          // Gaussians per preprocess / duplicate block
 constexpr int kSortThreads = 256;
 constexpr int kSortItems = 16;           // keys per thread per sort tile
@@ -116,7 +117,8 @@ struct BinningLayout {
     L.tvals0 = o; o = align_up(o + sizeof(uint32_t) * C);
     L.tvals1 = o; o = align_up(o + sizeof(uint32_t) * C);
     L.hist = o; o = align_up(o + sizeof(uint32_t) * kMaxSortPasses * kRadix);
-    L.tile_lookback = o; o = align_up(o + sizeof(uint32_t) * kTilePasses * sort_tiles(C) * kRadix);
+    // room for a per-view tile sort of a batch: up to kMaxBatchViews more (partial) tiles per pass
+    L.tile_lookback = o; o = align_up(o + sizeof(uint32_t) * kTilePasses * (sort_tiles(C) + kMaxBatchViews) * kRadix);
     L.total = o;
     return L;
   }
@@ -139,23 +141,28 @@ struct BinningLayout {
 // BinningLayout buffer as in the single-view case).  Per-(view, Gaussian) arrays are view-major;
 // per-pixel arrays hold the views' pixels back to back, ranges the views' tiles back to back.
 //
-//   header | instances per view u64[32] | duplicate-scan look-back u64[VP/256] |
+//   header | instances per view u64[32] | view tile bases u32[32] | duplicate-scan look-back u64[VP/256] |
 //   depth-sort look-back u32[4][V sort tiles(P)][256] | depth histograms u32[V][4][256] |
+//   tile-sort histograms u32[V][3][256] |
 //   radii i32[VP] | splat records float4[2VP] | colour float4[VP] | depth f32[VP] |
 //   depth-sort keys/values u32[4][VP] | gradient accumulators float4[3VP] |
 //   final transmittance f32[pixels] | last contributor u32[pixels] | tile ranges uint2[tiles]
 struct BatchLayout {
-  size_t header, view_rendered, dup_scan, depth_lookback, depth_hist, zero_end, radii, splat, color, depth,
+  size_t header, view_rendered, view_key_base, dup_scan, depth_lookback, depth_hist, tile_hist, zero_end, radii, splat, color, depth,
       dkeys0, dkeys1, dvals0, dvals1, grad_acc, final_T, n_contrib, ranges, total;
   static BatchLayout make(int64_t P, int V, int64_t pixels, int64_t tiles) {
     BatchLayout L;
     const int64_t R = P * V;
     size_t o = 0;
     L.header = o; o = align_up(o + sizeof(GeomHeader));
-    L.view_rendered = o; o = align_up(o + sizeof(uint64_t) * 32);
+    // the view tile bases directly follow the per-view counts: the tile sort finds them there
+    static_assert(sizeof(uint64_t) * kMaxBatchViews % kAlign == 0, "view_key_base must follow view_rendered");
+    L.view_rendered = o; o = align_up(o + sizeof(uint64_t) * kMaxBatchViews);
+    L.view_key_base = o; o = align_up(o + sizeof(uint32_t) * kMaxBatchViews);
     L.dup_scan = o; o = align_up(o + sizeof(uint64_t) * ((R + kScanBlock - 1) / kScanBlock));
     L.depth_lookback = o; o = align_up(o + sizeof(uint32_t) * kDepthPasses * sort_tiles(P) * V * kRadix);
     L.depth_hist = o; o = align_up(o + sizeof(uint32_t) * V * kDepthPasses * kRadix);
+    L.tile_hist = o; o = align_up(o + sizeof(uint32_t) * V * kTilePasses * kRadix);
     L.zero_end = o;  // everything above is cleared before each pass
     L.radii = o; o = align_up(o + sizeof(int32_t) * R);
     L.splat = o; o = align_up(o + sizeof(float) * 8 * R);

@@ -52,10 +52,18 @@ def _batch(gt, views, dpix_list, bg, fp64_poles=False, capacity=None):
     return images, per_view, state, grads
 
 
+# Four 3072x1536 views and one 512x256 hold 74,240 tiles: global tile ids need 17 bits (three sort
+# passes), view-local ones 15 (two), so the tile sort runs per view; with P = 200 (< 256) the batch
+# falls back to the global tile sort.
+PER_VIEW_SIZES = [(3072, 1536)] * 4 + [(512, 256)]
+
+
 @pytest.mark.parametrize("sizes,P,seed", [
     ([(512, 256)], 10_000, 0),
     ([(512, 256), (1024, 512), (96, 48), (500, 250)], 20_000, 1),
     ([(2048, 1024), (512, 256), (3072, 1536)], 60_000, 2),
+    (PER_VIEW_SIZES, 20_000, 5),
+    (PER_VIEW_SIZES, 200, 6),
 ])
 def test_batch_matches_single_views(cuda, sizes, P, seed):
     g = scenes.make_gaussians(P, seed=seed)
@@ -117,10 +125,12 @@ def test_bf16_sh_equals_fp32_path_on_rounded_coefficients(cuda):
         assert _rel(getattr(out["bf16"][2], k), getattr(out["fp32"][2], k)) < GRAD_RTOL, k
 
 
-def test_capacity_overflow_resumes(cuda):
+@pytest.mark.parametrize("sizes", [[(512, 256), (256, 128)], PER_VIEW_SIZES])
+def test_capacity_overflow_resumes(cuda, sizes):
     g = scenes.make_gaussians(10_000, seed=4)
     gt = lonlat.GaussianTensors.from_numpy(g)
-    views = [scenes.identity_view(512, 256), scenes.make_view(256, 128, (0.5, 0.0, 0.0))]
+    views = [scenes.identity_view(*sizes[0])] + [scenes.make_view(w, h, (0.5, 0.1 * i, 0.0))
+                                                 for i, (w, h) in enumerate(sizes[1:])]
     cams = batch.BatchCameras.from_views(views)
     ref_images, ref_per, _ = batch.render_batch(gt, cams)
     small = batch.BatchState(gt.P, cams.sizes, capacity=1000)
