@@ -11,7 +11,9 @@
 //  2. duplicate: instances are emitted walking the Gaussians in that order, each block scanning
 //     its Gaussians' tile counts and joining a decoupled look-back for its output offset, and
 //     counting the digits of the keys it writes for the tile sort;
-//  3. tile sort: a stable LSD radix sort (2 onesweep passes) of the instances by tile id only.
+//  3. tile sort: a stable LSD radix sort (2 onesweep passes) of the instances by tile id only
+//     (for a batch of views, per view on view-local tile ids when those need fewer passes than
+//     the batch's global ids: each view's instances are contiguous after step 2).
 // Stability makes (1)+(3) equal to the reference's single sort: instance passes drop from six
 // over 12-byte items to two over 8-byte items; the four depth passes run over P, not R, items.
 //  4. ranges: per-tile [start, end) over the sorted tile ids.
