@@ -368,6 +368,9 @@ __global__ void __launch_bounds__(256) adam_gaussian_kernel(const __grid_constan
   // kAdamUnroll elements before updating any, so that many loads are in flight per thread.
   constexpr int kAdamUnroll = 4;
   const uint32_t per = (uint32_t)(M - 1) * 3u;
+  // e / per as a multiply-high by ceil(2^32 / per): for every 32-bit e the estimate is the quotient
+  // or one more, and one comparison settles it
+  const uint32_t per_magic = per ? (uint32_t)((0x100000000ull + per - 1) / per) : 0u;
   const AdamScalars& s = s_sc[2];
   for (int64_t base = (int64_t)blockIdx.x * blockDim.x * kAdamUnroll + threadIdx.x; base < rest_n;
        base += stride * kAdamUnroll) {
@@ -377,7 +380,9 @@ __global__ void __launch_bounds__(256) adam_gaussian_kernel(const __grid_constan
     for (int u = 0; u < kAdamUnroll; ++u) {
       const int64_t e = base + (int64_t)u * blockDim.x;
       if (e < rest_n) {
-        const uint32_t g = (uint32_t)e / per, r = (uint32_t)e - g * per;
+        uint32_t g = __umulhi((uint32_t)e, per_magic);
+        if ((uint64_t)g * per > (uint64_t)e) --g;
+        const uint32_t r = (uint32_t)e - g * per;
         sh_idx[u] = (size_t)g * M * 3 + 3 + r;
         pv[u] = p.prm.features_rest[e];
         mv[u] = p.st.m_rest[e];
