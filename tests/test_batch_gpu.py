@@ -298,3 +298,36 @@ def test_seam_wrap_changes_nothing_away_from_the_seam(cuda):
     b, pb, _ = batch.render_batch(gt, cams, seam_wrap=True)
     assert pa == pb
     torch.testing.assert_close(a[0], b[0], rtol=0, atol=0)
+
+
+def test_per_view_tile_sort_with_seam_wrap_matches_one_view_batches(cuda):
+    """The per-view tile sort (PER_VIEW_SIZES) with seam wrapping: every view of the batch equals the
+    same view rendered as a batch of one (whose tile sort is the global one) -- instance counts,
+    last contributors, transmittance and image bit for bit, gradients to FP32 summation order."""
+    P = 20_000
+    g = scenes.make_gaussians(P, seed=17)
+    gt = lonlat.GaussianTensors.from_numpy(g)
+    views = _views(PER_VIEW_SIZES, 17)
+    cams = batch.BatchCameras.from_views(views)
+    imgs, per, state = batch.render_batch(gt, cams, seam_wrap=True)
+    dl = [torch.from_numpy(scenes.upstream_grad(v.width, v.height, seed=60 + i)).cuda() for i, v in enumerate(views)]
+    grads = batch.BatchGradients.empty(gt.P, gt.M, cuda)
+    state.backward(gt, cams, dl, grads, seam_wrap=True)
+    torch.cuda.synchronize()
+    sv = state.state_view()
+    sums = {k: 0.0 for k in ("dL_dmeans3D", "dL_dsh", "dL_dopacity")}
+    for v, view in enumerate(views):
+        one = batch.BatchCameras.from_views([view])
+        img1, per1, st1 = batch.render_batch(gt, one, seam_wrap=True)
+        g1 = batch.BatchGradients.empty(gt.P, gt.M, cuda)
+        st1.backward(gt, one, [dl[v]], g1, seam_wrap=True)
+        torch.cuda.synchronize()
+        sv1 = st1.state_view()
+        assert per[v] == per1[0]
+        torch.testing.assert_close(sv["n_contrib"][v], sv1["n_contrib"][0], rtol=0, atol=0)
+        torch.testing.assert_close(sv["final_T"][v], sv1["final_T"][0], rtol=0, atol=0)
+        torch.testing.assert_close(imgs[v], img1[0], rtol=0, atol=0)
+        for k in sums:
+            sums[k] = sums[k] + getattr(g1, k).double()
+    for k, ref in sums.items():
+        assert _rel(getattr(grads, k), ref) < GRAD_RTOL, k
