@@ -47,72 +47,9 @@ struct LossParams {
   float w[kWin];
 };
 
-// Separable 11-tap convolution with zero padding of a [rows][W] plane region into the tile at
-// (x0, y0); `src(ok, y, x, v)` gives the NQ inputs at (y, x) (zeros when !ok, i.e. outside
-// [0, rows) x [0, W)), `out(y, x, v)` receives the NQ convolved values of an output pixel.  Each
-// pass slides an 11-tap window along a register segment (kSeg outputs from kSeg + 10 loads), so
-// shared memory is read ~1.8 times per output instead of 11 times.
+// Register segment of the sliding 11-tap windows: kSeg outputs from kSeg + 10 loads, so shared
+// memory is read ~1.8 times per output instead of 11 times.
 constexpr int kSeg = 8;
-template <int NQ, class Src, class Out>
-__device__ __forceinline__ void conv_tile(int x0, int y0, int rows, int W, const float* w,
-                                          float (*in)[kLossTileH + 2 * kHalf][kLossTileW + 2 * kHalf],
-                                          float (*tmp)[kLossTileH + 2 * kHalf][kLossTileW], Src src, Out out) {
-  constexpr int IH = kLossTileH + 2 * kHalf, IW = kLossTileW + 2 * kHalf;
-  constexpr int kRowsPerPass = kLossThreads / kLossTileW;  // 8 rows of 32 threads
-  const int lx = threadIdx.x % kLossTileW, ly = threadIdx.x / kLossTileW;
-  for (int ty = ly; ty < IH; ty += kRowsPerPass) {
-    for (int tx = lx; tx < IW; tx += kLossTileW) {
-      const int y = y0 + ty - kHalf, x = x0 + tx - kHalf;
-      const bool ok = y >= 0 && y < rows && x >= 0 && x < W;
-      float v[NQ];
-      src(ok, y, x, v);
-#pragma unroll
-      for (int q = 0; q < NQ; ++q) in[q][ty][tx] = v[q];
-    }
-  }
-  __syncthreads();
-  // horizontal: task = (q, row, segment of kSeg output columns)
-  constexpr int kHSegs = kLossTileW / kSeg;
-  for (int t = threadIdx.x; t < NQ * IH * kHSegs; t += kLossThreads) {
-    const int q = t / (IH * kHSegs), rem = t - q * (IH * kHSegs);
-    const int ty = rem / kHSegs, xs = (rem - ty * kHSegs) * kSeg;
-    float r[kSeg + kWin - 1];
-#pragma unroll
-    for (int k = 0; k < kSeg + kWin - 1; ++k) r[k] = in[q][ty][xs + k];
-#pragma unroll
-    for (int j = 0; j < kSeg; ++j) {
-      float acc = 0.f;
-#pragma unroll
-      for (int k = 0; k < kWin; ++k) acc = fmaf(w[k], r[j + k], acc);
-      tmp[q][ty][xs + j] = acc;
-    }
-  }
-  __syncthreads();
-  // vertical: task = (q, column, segment of kSeg output rows); results reuse `in`
-  constexpr int kVSegs = kLossTileH / kSeg;
-  for (int t = threadIdx.x; t < NQ * kLossTileW * kVSegs; t += kLossThreads) {
-    const int q = t / (kLossTileW * kVSegs), rem = t - q * (kLossTileW * kVSegs);
-    const int ys = (rem / kLossTileW) * kSeg, tx = rem % kLossTileW;
-    float r[kSeg + kWin - 1];
-#pragma unroll
-    for (int k = 0; k < kSeg + kWin - 1; ++k) r[k] = tmp[q][ys + k][tx];
-#pragma unroll
-    for (int j = 0; j < kSeg; ++j) {
-      float acc = 0.f;
-#pragma unroll
-      for (int k = 0; k < kWin; ++k) acc = fmaf(w[k], r[j + k], acc);
-      in[q][ys + j][tx] = acc;
-    }
-  }
-  __syncthreads();
-  for (int ty = ly; ty < kLossTileH; ty += kRowsPerPass) {
-    float v[NQ];
-#pragma unroll
-    for (int q = 0; q < NQ; ++q) v[q] = in[q][ty][lx];
-    const int y = y0 + ty, x = x0 + lx;
-    if (y < rows && x < W) out(y, x, v);
-  }
-}
 
 // Block sums of (a, b) into partials[2 * block] (no contended atomics; loss_finalize adds them).
 __device__ __forceinline__ void block_sum2(double a, double b, double* partials) {
@@ -140,13 +77,102 @@ __device__ __forceinline__ void block_sum2(double a, double b, double* partials)
   }
 }
 
-// Kernel 1: local statistics of one tile of one channel (blockIdx.z).
+// Separable 11-tap convolution with zero padding of a [rows][W] plane region, by column strips: a
+// block walks down kStripChunks chunks of 16 output rows of a 32-column strip, each pass sliding
+// the window along register segments, and keeps the horizontal pass's last 10 rows for the next
+// chunk, so each input row is loaded and filtered horizontally once per strip (a 16x32 tile with
+// its own 26-row window re-read 10 halo rows: 0.228 -> 0.213 ms per 2048x1024x3 loss, identical
+// results).
+// `src(ok, y, x, v)` gives the NQ inputs at (y, x) (zeros when !ok, i.e. outside [0, rows) x
+// [0, W)), `out(y, x, v)` receives the NQ convolved values of an output pixel; `s_in` holds up to
+// 16 input rows (later the vertical results), `s_tmp` the horizontal results of input rows
+// y0 - 5 .. y0 + 20 of the current chunk.
+constexpr int kStripChunks = 4;
+constexpr int kStripRows = kStripChunks * kLossTileH;
+
+template <int NQ, class Src, class Out>
+__device__ __forceinline__ void conv_strip(int x0, int ystart, int rows, int W, const float* w,
+                                           float (*s_in)[kLossTileH][kLossTileW + 2 * kHalf],
+                                           float (*s_tmp)[kLossTileH + 2 * kHalf][kLossTileW], Src src, Out out) {
+  constexpr int IW = kLossTileW + 2 * kHalf;
+  constexpr int kRowsPerPass = kLossThreads / kLossTileW;
+  constexpr int kHSegs = kLossTileW / kSeg, kVSegs = kLossTileH / kSeg;
+  const int lx = threadIdx.x % kLossTileW, ly = threadIdx.x / kLossTileW;
+  // input rows [ya, ya + n) (with the x halo) into s_in rows [0, n), their horizontal pass into
+  // s_tmp rows [dst, dst + n)
+  auto load_and_filter = [&](int ya, int n, int dst) {
+    for (int ty = ly; ty < n; ty += kRowsPerPass) {
+      for (int tx = lx; tx < IW; tx += kLossTileW) {
+        const int y = ya + ty, x = x0 + tx - kHalf;
+        const bool ok = y >= 0 && y < rows && x >= 0 && x < W;
+        float v[NQ];
+        src(ok, y, x, v);
+#pragma unroll
+        for (int q = 0; q < NQ; ++q) s_in[q][ty][tx] = v[q];
+      }
+    }
+    __syncthreads();
+    for (int t = threadIdx.x; t < NQ * n * kHSegs; t += kLossThreads) {
+      const int q = t / (n * kHSegs), rem = t - q * (n * kHSegs);
+      const int ty = rem / kHSegs, xs = (rem - ty * kHSegs) * kSeg;
+      float r[kSeg + kWin - 1];
+#pragma unroll
+      for (int k = 0; k < kSeg + kWin - 1; ++k) r[k] = s_in[q][ty][xs + k];
+#pragma unroll
+      for (int j = 0; j < kSeg; ++j) {
+        float acc = 0.f;
+#pragma unroll
+        for (int k = 0; k < kWin; ++k) acc = fmaf(w[k], r[j + k], acc);
+        s_tmp[q][dst + ty][xs + j] = acc;
+      }
+    }
+    __syncthreads();
+  };
+
+  load_and_filter(ystart - kHalf, 2 * kHalf, 0);  // rows ystart - 5 .. ystart + 4
+  for (int ch = 0; ch < kStripChunks; ++ch) {
+    const int y0 = ystart + ch * kLossTileH;
+    if (y0 >= rows) break;  // block-uniform
+    load_and_filter(y0 + kHalf, kLossTileH, 2 * kHalf);  // rows y0 + 5 .. y0 + 20
+    // vertical pass of the chunk's 16 output rows into s_in
+    for (int t = threadIdx.x; t < NQ * kLossTileW * kVSegs; t += kLossThreads) {
+      const int q = t / (kLossTileW * kVSegs), rem = t - q * (kLossTileW * kVSegs);
+      const int ys = (rem / kLossTileW) * kSeg, tx = rem % kLossTileW;
+      float r[kSeg + kWin - 1];
+#pragma unroll
+      for (int k = 0; k < kSeg + kWin - 1; ++k) r[k] = s_tmp[q][ys + k][tx];
+#pragma unroll
+      for (int j = 0; j < kSeg; ++j) {
+        float acc = 0.f;
+#pragma unroll
+        for (int k = 0; k < kWin; ++k) acc = fmaf(w[k], r[j + k], acc);
+        s_in[q][ys + j][tx] = acc;
+      }
+    }
+    __syncthreads();
+    // outputs of the chunk; meanwhile the horizontal rows the next chunk shares move to the front
+    for (int ty = ly; ty < kLossTileH; ty += kRowsPerPass) {
+      float v[NQ];
+#pragma unroll
+      for (int q = 0; q < NQ; ++q) v[q] = s_in[q][ty][lx];
+      const int y = y0 + ty, x = x0 + lx;
+      if (y < rows && x < W) out(y, x, v);
+    }
+    for (int t = threadIdx.x; t < NQ * 2 * kHalf * kLossTileW; t += kLossThreads) {
+      const int q = t / (2 * kHalf * kLossTileW), rem = t - q * (2 * kHalf * kLossTileW);
+      const int r = rem / kLossTileW, x = rem - r * kLossTileW;
+      s_tmp[q][r][x] = s_tmp[q][kLossTileH + r][x];
+    }
+    __syncthreads();
+  }
+}
+
+// Kernel 1: local statistics of one 32-column strip of kStripRows rows of one channel (blockIdx.z).
 __global__ void __launch_bounds__(kLossThreads) ssim_stats_kernel(const __grid_constant__ LossParams p) {
-  constexpr int IH = kLossTileH + 2 * kHalf, IW = kLossTileW + 2 * kHalf;
-  __shared__ float s_in[5][IH][IW];
-  __shared__ float s_tmp[5][IH][kLossTileW];
+  __shared__ float s_in[5][kLossTileH][kLossTileW + 2 * kHalf];
+  __shared__ float s_tmp[5][kLossTileH + 2 * kHalf][kLossTileW];
   const int c = blockIdx.z;
-  const int x0 = blockIdx.x * kLossTileW, y0 = blockIdx.y * kLossTileH;
+  const int x0 = blockIdx.x * kLossTileW, ystart = blockIdx.y * kStripRows;
   const size_t plane = (size_t)p.H * p.W;
   const float* a = p.img + c * plane;
   const float* b = p.gt + c * plane;
@@ -180,17 +206,16 @@ __global__ void __launch_bounds__(kLossThreads) ssim_stats_kernel(const __grid_c
     ssum += (double)S;
     l1 += (double)fabsf(a[o] - b[o]);
   };
-  conv_tile<5>(x0, y0, p.rows, p.W, p.w, s_in, s_tmp, src, out);
+  conv_strip<5>(x0, ystart, p.rows, p.W, p.w, s_in, s_tmp, src, out);
   block_sum2(l1, ssum, p.sums);
 }
 
-// Kernel 2: dL/dimg of one tile of one channel.
+// Kernel 2: dL/dimg of one 32-column strip of kStripRows rows of one channel.
 __global__ void __launch_bounds__(kLossThreads) ssim_grad_kernel(const __grid_constant__ LossParams p) {
-  constexpr int IH = kLossTileH + 2 * kHalf, IW = kLossTileW + 2 * kHalf;
-  __shared__ float s_in[3][IH][IW];
-  __shared__ float s_tmp[3][IH][kLossTileW];
+  __shared__ float s_in[3][kLossTileH][kLossTileW + 2 * kHalf];
+  __shared__ float s_tmp[3][kLossTileH + 2 * kHalf][kLossTileW];
   const int c = blockIdx.z;
-  const int x0 = blockIdx.x * kLossTileW, y0 = blockIdx.y * kLossTileH;
+  const int x0 = blockIdx.x * kLossTileW, ystart = blockIdx.y * kStripRows;
   const size_t plane = (size_t)p.H * p.W;
   const float* a = p.img + c * plane;
   const float* b = p.gt + c * plane;
@@ -215,7 +240,7 @@ __global__ void __launch_bounds__(kLossThreads) ssim_grad_kernel(const __grid_co
     const float dssim = m[0] + 2.f * u * m[1] + g * m[2];
     d[o] = k_l1 * sgn + k_ssim * dssim;
   };
-  conv_tile<3>(x0, y0, p.rows, p.W, p.w, s_in, s_tmp, src, out);
+  conv_strip<3>(x0, ystart, p.rows, p.W, p.w, s_in, s_tmp, src, out);
   // rows below `rows` are not part of the loss
   if (blockIdx.y == gridDim.y - 1) {
     for (int i = threadIdx.x; i < (p.H - p.rows) * kLossTileW; i += blockDim.x) {
@@ -498,10 +523,11 @@ int omnigs_l1_dssim(const float* image, const float* gt, int C, int H, int W, in
     sum += p.w[k];
   }
   for (int k = 0; k < kWin; ++k) p.w[k] /= sum;
-  const int blocks = (int)(grid.x * grid.y * grid.z);
+  const dim3 strip_grid(grid.x, (rows + kStripRows - 1) / kStripRows, C);
+  const int blocks = (int)(strip_grid.x * strip_grid.y * strip_grid.z);
   staged(OMNIGS_STAGE_OTHER, 3, s, [&] {
-    ssim_stats_kernel<<<grid, kLossThreads, 0, s>>>(p);
-    ssim_grad_kernel<<<grid, kLossThreads, 0, s>>>(p);
+    ssim_stats_kernel<<<strip_grid, kLossThreads, 0, s>>>(p);
+    ssim_grad_kernel<<<strip_grid, kLossThreads, 0, s>>>(p);
     loss_finalize_kernel<<<1, 1024, 0, s>>>(p.sums, blocks, loss, 1.0 / ((double)C * rows * W), lambda_dssim);
   });
   return check_launch("l1 + d-ssim");
