@@ -1,5 +1,5 @@
 // Shared pieces of the forward and backward tile blends: the pixel patch a warp owns, the
-// alpha-support box test against it, and the staging of a batch of splats into shared memory.
+// alpha-support test of a splat against it, and the staging of a batch of splats into shared memory.
 #pragma once
 
 #include "device_util.cuh"
@@ -47,10 +47,14 @@ __device__ __forceinline__ uint2 checked_range(const uint2* ranges, uint32_t til
   return range;
 }
 
+// Rows of the patch a warp owns (8 columns wide).
+constexpr int kPatchRows = 4 * kBlendPx;
+
 struct BlendPatch {
   int px, py0;       // this thread's column and first row
   float pxf;         // column as float
-  float wcx, wcy;    // centre of the warp's patch
+  float wx0, wy0;    // first column and row of the warp's patch
+  float wcx;         // centre column of the warp's patch
   float wrap_w;      // image width in seam-wrapping mode, else 0
 
   // x of the splat's copy (shifted by a multiple of the image width) nearest this patch; the
@@ -64,13 +68,14 @@ struct BlendPatch {
   static __device__ __forceinline__ BlendPatch make(int tile_x, int tile_y, float wrap_w = 0.f) {
     const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
     const int wx0 = tile_x * 16 + (warp & 1) * 8;
-    const int wy0 = tile_y * 16 + (warp >> 1) * 4 * kBlendPx;
+    const int wy0 = tile_y * 16 + (warp >> 1) * kPatchRows;
     BlendPatch b;
     b.px = wx0 + (lane & 7);
     b.py0 = wy0 + (lane >> 3);
     b.pxf = (float)b.px;
+    b.wx0 = (float)wx0;
+    b.wy0 = (float)wy0;
     b.wcx = (float)wx0 + 3.5f;
-    b.wcy = (float)wy0 + 0.5f * (4 * kBlendPx - 1);
     b.wrap_w = wrap_w;
     return b;
   }
@@ -78,11 +83,30 @@ struct BlendPatch {
   __device__ __forceinline__ float pyf(int i) const { return (float)(py0 + 4 * i); }
   __device__ __forceinline__ bool inside(int i, int W, int H) const { return px < W && py(i) < H; }
   __device__ __forceinline__ int64_t pixel(int i, int W) const { return (int64_t)py(i) * W + px; }
-  // The splat's alpha-support box (centre a.xy, half extents b.zw) touches the patch.  Written as
-  // a negated "misses" test so that NaN extents count as touching (the per-pixel test decides).
+
+  // Whether the splat (a = {x, y, conic a, conic b}, b = {conic c, opacity, thr, det}) can reach
+  // alpha >= 1/255 at some pixel centre of the patch: the minimum of its quadratic form
+  // q(d) = a dx^2 + 2 b dx dy + c dy^2 over the patch's offsets d = centre - pixel, a rectangle
+  // [dxl, dxh] x [dyl, dyh], against thr.  A convex form's minimum over a rectangle that does not
+  // contain its centre lies on a side facing the centre (KKT), so two candidate sides suffice: the
+  // column side at dxn (the x offset nearest 0) minimised over dy, and the row side at dyn minimised
+  // over dx.  Scaled by c (resp. a) each is a clamp and a sum of squares without division:
+  //   c q(dxn, dy) = (c dy + b dxn)^2 + det dxn^2, minimised at c dy = clamp(-b dxn, c dyl, c dyh).
+  // When the centre lies inside the patch both offsets are 0 and the value is 0.  Any other side
+  // value is q at a point of the patch, so it never claims a miss wrongly.  Written as a negated
+  // "misses" test so that NaN (det of a non-positive-definite conic, non-finite inputs) hits: the
+  // per-pixel test decides.
   template <bool kWrap>
   __device__ __forceinline__ bool hit(const float4& a, const float4& b) const {
-    return !(fabsf(center_x<kWrap>(a.x) - wcx) > b.z + 3.5f || fabsf(a.y - wcy) > b.w + (2.0f * kBlendPx - 0.5f));
+    const float dxh = center_x<kWrap>(a.x) - wx0, dxl = dxh - 7.0f;
+    const float dyh = a.y - wy0, dyl = dyh - (float)(kPatchRows - 1);
+    const float dxn = fminf(fmaxf(dxl, 0.0f), dxh), dyn = fminf(fmaxf(dyl, 0.0f), dyh);
+    const float bx = a.w * dxn, by = a.w * dyn;
+    const float sx = fminf(fmaxf(-bx, b.x * dyl), b.x * dyh) + bx;
+    const float sy = fminf(fmaxf(-by, a.z * dxl), a.z * dxh) + by;
+    const float vx = fmaf(sx, sx, b.w * dxn * dxn);
+    const float vy = fmaf(sy, sy, b.w * dyn * dyn);
+    return !(vx > b.x * b.z && vy > a.z * b.z);
   }
 };
 

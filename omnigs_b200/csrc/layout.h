@@ -7,7 +7,7 @@
 //   geometry (per Gaussian, P):  header | duplicate-scan look-back u64[P/256] |
 //                                depth-sort look-back u32[4][sort tiles][256] |
 //                                splat records float4[2P] {x, y, conic a, b}
-//                                {conic c, opacity, cull half-width, cull half-height} |
+//                                {conic c, opacity, cull threshold, conic determinant} |
 //                                colour float4[P] {r, g, b, clamp bits} | depth f32[P] |
 //                                tiles_touched u32[P] | depth-sort keys/values u32[4][P] |
 //                                gradient accumulators float4[3P]

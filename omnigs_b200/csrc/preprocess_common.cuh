@@ -3,9 +3,9 @@
 //
 // Evaluates the reference's FP32 sequence (forward.cu:592-703): near cull at r^2 <= 0.04,
 // equirect projection, 2D covariance through the lonlat Jacobian, conic, radius, clamped tile rect
-// and SH colour.  Besides the reference's outputs, each visible splat gets the half-extents of the
-// axis-aligned box outside which its alpha is provably below 1/255; the blend kernels use them to
-// skip a splat for a whole warp without changing any per-pixel decision.
+// and SH colour.  Besides the reference's outputs, each visible splat gets the threshold of its
+// quadratic form beyond which its alpha is provably below 1/255, and the conic's determinant; the
+// blend kernels use them to skip a splat for a whole warp without changing any per-pixel decision.
 #pragma once
 
 #include "device_util.cuh"
@@ -13,24 +13,28 @@
 
 namespace omnigs {
 
-// Half-extents (pixels) of the box that contains every pixel where o * exp(power) can reach the
-// reference's 1/255 skip threshold (forward.cu:436-438).  power = -d^T Q d / 2 with Q the conic,
-// so alpha >= 1/255 needs d^T Q d <= 2 tau, tau = ln(255 o) (+0.01 slack for expf error and FP32
-// rounding of `power`).  The ellipse's x half-extent is sqrt(2 tau (Q^-1)_xx).  Non-finite inputs
-// or an indefinite conic disable culling (+inf); an opacity that can never reach 1/255 culls
-// everywhere (-inf).
-__device__ __forceinline__ float2 cull_half_extent(float a, float b, float c, float o) {
-  const float inf = __int_as_float(0x7f800000);
-  if (!(isfinite(a) && isfinite(b) && isfinite(c) && isfinite(o))) return make_float2(inf, inf);
-  if (!(o > 0.0f)) return make_float2(-inf, -inf);
+// Alpha-support quadric of a splat: {thr, det} such that o * exp(power) can reach the reference's
+// 1/255 skip threshold (forward.cu:436-438) only where d^T Q d <= thr, Q = [a b; b c] the conic and
+// d = centre - pixel (power = -d^T Q d / 2).  Exactly, alpha >= 1/255 needs d^T Q d <= 2 tau with
+// tau = ln(255 o); thr adds 0.01 to tau (expf error, FP32 rounding of `power`) and a relative
+// 1e-5 a c / det, which grows with the ellipse's elongation like the cancellation error of the
+// blends' FP32 evaluation of `power` (its terms reach 2 tau a c / det on the ellipse), rounded up.
+// det = a c - b^2 is exact in FP64 from the float conic and rounded down.  Both err towards "the
+// splat may contribute".  Non-finite inputs or a conic that is not positive definite give
+// det = NaN (every patch test hits: the per-pixel test decides); an opacity that can never reach
+// 1/255 gives thr = -inf (no patch test hits).
+__device__ __forceinline__ float2 cull_quadric(float x, float y, float a, float b, float c, float o) {
+  const float inf = __int_as_float(0x7f800000), nan = __int_as_float(0x7fffffff);
+  if (!(isfinite(x) && isfinite(y) && isfinite(a) && isfinite(b) && isfinite(c) && isfinite(o)))
+    return make_float2(inf, nan);
+  if (!(o > 0.0f)) return make_float2(-inf, 1.0f);
   const double tau = log(255.0 * (double)o) + 0.01;
-  if (tau <= 0.0) return make_float2(-inf, -inf);
+  if (tau <= 0.0) return make_float2(-inf, 1.0f);
   const double A = a, B = b, C = c;
   const double det = A * C - B * B;
-  if (!(A > 0.0) || !(det > 0.0)) return make_float2(inf, inf);
-  const double hx = sqrt(2.0 * tau * C / det) * (1.0 + 1e-4) + 1e-2;
-  const double hy = sqrt(2.0 * tau * A / det) * (1.0 + 1e-4) + 1e-2;
-  return make_float2(__double2float_ru(hx), __double2float_ru(hy));
+  if (!(A > 0.0) || !(C > 0.0) || !(det > 0.0)) return make_float2(inf, nan);
+  const double thr = 2.0 * tau * (1.0 + 1e-5 * (A * C / det));
+  return make_float2(__double2float_ru(thr), __double2float_rd(det));
 }
 
 // One splat of one view.  radius == 0 means culled; then only depth_key (+inf, so culled
@@ -40,7 +44,7 @@ struct SplatResult {
   uint32_t touched;
   float depth_key;
   float4 s0;   // x, y, conic a, conic b
-  float4 s1;   // conic c, opacity, cull half-width, cull half-height
+  float4 s1;   // conic c, opacity, cull threshold, conic determinant
   float4 col;  // r, g, b, clamp bits
 };
 
@@ -120,9 +124,9 @@ __device__ __forceinline__ SplatResult preprocess_splat(float3 p_orig, const flo
   } else {
     res.col = make_float4(color_precomp[0], color_precomp[1], color_precomp[2], __uint_as_float(0u));
   }
-  const float2 ext = cull_half_extent(conic.x, conic.y, conic.z, opacity);
+  const float2 cull = cull_quadric(point_image.x, point_image.y, conic.x, conic.y, conic.z, opacity);
   res.s0 = make_float4(point_image.x, point_image.y, conic.x, conic.y);
-  res.s1 = make_float4(conic.z, opacity, ext.x, ext.y);
+  res.s1 = make_float4(conic.z, opacity, cull.x, cull.y);
   res.depth_key = r;
   res.radius = radius;
   res.touched = area;

@@ -14,7 +14,7 @@
 // pixels and writes the 9 sums to its warp's shared buffer; every second contributing splat the
 // warp that owns the 8 x 8 patch reduces the buffer transposed (one lane per splat and value, 32
 // terms each) and adds the accumulator records with one atomic per value.  Warps skip splats
-// whose alpha-support box misses their patch or that lie behind all of their pixels' last
+// that cannot reach alpha >= 1/255 in their patch or that lie behind all of their pixels' last
 // contributors, and the block starts at the batch holding its largest last contributor instead of
 // at the end of the range.
 #include "blend_common.cuh"

@@ -8,8 +8,9 @@
 //    shared-memory reads, loop control and votes are paid once per thread, not once per pixel,
 //    and the two pixels' arithmetic runs in packed f32x2 instructions (each lane rounded exactly
 //    as the scalar operation, so results are unchanged);
-//  * for each staged batch a warp ballots which splats' alpha-support boxes (computed in the
-//    preprocess) touch its patch and iterates only over those, so pairs that the reference rejects
+//  * for each staged batch a warp ballots which splats can reach alpha >= 1/255 somewhere in its
+//    patch (the exact minimum of the splat's quadratic form over the patch against a threshold
+//    computed in the preprocess) and iterates only over those, so pairs that the reference rejects
 //    pixel by pixel are skipped a warp at a time;
 //  * a warp stops after the group of 32 candidate splats in which all of its pixels saturated
 //    (one warp vote per group; saturated pixels skip the per-splat work at once), and the block

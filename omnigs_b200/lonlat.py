@@ -199,7 +199,7 @@ class LonlatState:
         splat = _view_tensor(self.geom, v.splat, 8 * P, torch.float32).view(P, 8)
         color = _view_tensor(self.geom, v.color, 4 * P, torch.float32).view(P, 4)
         return dict(means2D=splat[:, 0:2], conic_opacity=torch.cat([splat[:, 2:5], splat[:, 5:6]], 1),
-                    cull_extent=splat[:, 6:8], rgb=color[:, :3],
+                    cull=splat[:, 6:8], rgb=color[:, :3],
                     clamp_bits=color[:, 3].view(torch.int32),
                     depths=_view_tensor(self.geom, v.depth, P, torch.float32),
                     tiles_touched=_view_tensor(self.geom, v.tiles_touched, P, torch.int32),
