@@ -176,8 +176,8 @@ class BatchState:
         return int(n.value), [int(x) for x in per], int(st.value)
 
     def state_view(self) -> dict:
-        """Device tensors aliasing the state: radii [V,P], splat [V,P,8], color [V,P,4], and per view
-        final_T / n_contrib [H*W] and ranges [tiles,2]."""
+        """Device tensors aliasing the state: radii [V,P], splat [V,P,8], color [V,P,4], depth [V,P],
+        and per view final_T / n_contrib [H*W] and ranges [tiles,2]."""
         sv = capi.BatchStateView()
         W = (ctypes.c_int * self.V)(*[w for w, _ in self.sizes])
         H = (ctypes.c_int * self.V)(*[h for _, h in self.sizes])
@@ -192,6 +192,7 @@ class BatchState:
         out = dict(radii=_view_tensor(self.state, sv.radii, V * P, torch.int32).view(V, P),
                    splat=_view_tensor(self.state, sv.splat, 8 * V * P, torch.float32).view(V, P, 8),
                    color=_view_tensor(self.state, sv.color, 4 * V * P, torch.float32).view(V, P, 4),
+                   depth=_view_tensor(self.state, sv.depth, V * P, torch.float32).view(V, P),
                    final_T=[], n_contrib=[], ranges=[], tile_base=[], pixel_base=[])
         for v, (w, h) in enumerate(self.sizes):
             pb, tb, nt = sv.pixel_base[v], sv.tile_base[v], ((w + 15) // 16) * ((h + 15) // 16)
@@ -201,6 +202,18 @@ class BatchState:
             out["tile_base"].append(int(tb))
             out["pixel_base"].append(int(pb))
         return out
+
+
+    def binning_view(self, num_rendered: int) -> dict:
+        """Sorted instance list of the last forward: global tile ids and record indices
+        (view * P + Gaussian), device tensors aliasing the binning buffer."""
+        bv = capi.BinningView()
+        W = (ctypes.c_int * self.V)(*[w for w, _ in self.sizes])
+        H = (ctypes.c_int * self.V)(*[h for _, h in self.sizes])
+        capi.check(capi.lib().omnigs_batch_binning_view(self.binning.data_ptr(), self.binning.numel(), self.P,
+                                                        self.V, W, H, ctypes.byref(bv)), "omnigs_batch_binning_view")
+        return dict(tile_ids=_view_tensor(self.binning, bv.tile_ids, num_rendered, torch.int32),
+                    point_list=_view_tensor(self.binning, bv.point_list, num_rendered, torch.int32))
 
 
 def set_blend_batch(forward: int, backward: int):

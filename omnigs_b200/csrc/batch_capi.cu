@@ -528,6 +528,22 @@ int omnigs_batch_state_view(const void* state, int P, int V, const int* W, const
     out->tile_base[v] = plan.tile_base[v];
   }
   out->tile_passes = batch_tile_sort(plan).digits.passes;
+  out->depth = at<float>(state, L.depth);
+  return OMNIGS_OK;
+}
+
+int omnigs_batch_binning_view(const void* binning, size_t binning_bytes, int P, int V, const int* W, const int* H,
+                              OmnigsLonlatBinningView* out) {
+  g_last_error.clear();
+  if (binning == nullptr || out == nullptr) return fail(OMNIGS_ERR_INVALID_ARGUMENT, "bad view arguments");
+  BatchPlan plan;
+  if (int rc = make_plan(P, V, W, H, plan)) return rc;
+  const int64_t capacity = BinningLayout::capacity_for(binning_bytes);
+  if (capacity < 0) return fail(OMNIGS_ERR_BUFFER_TOO_SMALL, "binning buffer too small");
+  const BinningLayout BL = BinningLayout::make(capacity);
+  const int fin = batch_tile_sort(plan).digits.passes & 1;
+  out->tile_ids = at<uint32_t>(binning, fin ? BL.tkeys1 : BL.tkeys0);
+  out->point_list = at<uint32_t>(binning, fin ? BL.tvals1 : BL.tvals0);
   return OMNIGS_OK;
 }
 

@@ -61,11 +61,15 @@ def _unit_vectors(rng: np.random.Generator, n: int) -> np.ndarray:
 
 
 def make_gaussians(P: int, seed: int = 0, pole_fraction: float = 0.0,
-                   pole_min_lat_deg: float = 80.0) -> Gaussians:
+                   pole_min_lat_deg: float = 80.0, seam_fraction: float = 0.0,
+                   seam_width_deg: float = 5.0) -> Gaussians:
     """Scene of ``P`` Gaussians around a camera at the origin.
 
     ``pole_fraction`` of the means are placed at |latitude| > ``pole_min_lat_deg`` (in the
     identity camera frame, latitude = asin(y / r)); the pole-heavy precision workload uses 0.3.
+    ``seam_fraction`` of the means are placed within ``seam_width_deg`` of longitude +-180 deg
+    (the equirect image's left/right edge) at |latitude| < 60 deg, so their splats straddle the
+    seam.  Both default to 0, which leaves the generator's draws unchanged.
     """
     rng = np.random.Generator(np.random.PCG64(seed))
     r = np.cbrt(rng.random(P) * (125.0 - 1.0) + 1.0)
@@ -80,6 +84,12 @@ def make_gaussians(P: int, seed: int = 0, pole_fraction: float = 0.0,
         pole_dirs = np.stack([cos_lat * np.sin(lon), sin_lat, cos_lat * np.cos(lon)], axis=1)
         sel = rng.permutation(P)[:n_pole]
         dirs[sel] = pole_dirs
+    n_seam = int(round(P * seam_fraction))
+    if n_seam > 0:
+        lon = math.pi + np.radians(rng.uniform(-seam_width_deg, seam_width_deg, n_seam))
+        lat = np.radians(rng.uniform(-60.0, 60.0, n_seam))
+        seam_dirs = np.stack([np.cos(lat) * np.sin(lon), np.sin(lat), np.cos(lat) * np.cos(lon)], axis=1)
+        dirs[rng.permutation(P)[:n_seam]] = seam_dirs
     means = (dirs * r[:, None]).astype(np.float32)
     scales = np.exp(rng.normal(math.log(0.02), 0.5, (P, 3))).astype(np.float32)
     q = rng.standard_normal((P, 4))

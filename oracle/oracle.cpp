@@ -20,8 +20,9 @@
 // The glm expressions of the reference are restated with a small column-major double matrix type
 // (DMat3 below) so each formula can be read against its source line.
 //
-// Parity pin: checked against outputs of the reference CUDA rasterizer itself (rebuilt from its
-// sources for sm_100a and run on a B200) in tests/golden/, see tests/test_oracle_golden.py.
+// Parity pin: checked stage by stage against the reference CUDA rasterizer itself (rebuilt from its
+// own sources for sm_100a by oracle/ref/Makefile and run on a B200), each stage fed with the
+// reference's float intermediates: tests/test_oracle_vs_reference_gpu.py.
 
 #include <algorithm>
 #include <atomic>
@@ -140,6 +141,40 @@ inline void get_rect(T px, T py, int max_radius, int gx, int gy, int rmin[2], in
   rmax[1] = std::min(gy, std::max(0, to_int_sat((double)((py + r + b - (T)1) / b))));
 }
 
+// Seam-wrapping mode (an extension beyond the reference's lonlat path, which clamps): the tile
+// column range of getRectCyclic (auxiliary.h:68-83: x may start at -gx and end at 2 gx, columns
+// outside [0, gx) wrap modulo gx), with two choices of this package stated here as the mode's
+// semantics: the left edge is floor((x - r) / 16) rather than the truncation towards zero, so a
+// splat reaching less than one tile past x = 0 still gets the wrapped column, and the range is
+// capped at one image width (gx columns), so no tile holds a splat twice.  Rows clamp as getRect.
+template <class T>
+inline void get_rect_cyclic(T px, T py, int max_radius, int gx, int gy, int rmin[2], int rmax[2]) {
+  const T r = (T)max_radius;
+  const T b = (T)kTile;
+  rmin[0] = std::min(gx, std::max(-gx, to_int_sat(std::floor((double)((px - r) / b)))));
+  rmin[1] = std::min(gy, std::max(0, to_int_sat((double)((py - r) / b))));
+  rmax[0] = std::min(2 * gx, std::max(0, to_int_sat((double)((px + r + b - (T)1) / b))));
+  rmax[1] = std::min(gy, std::max(0, to_int_sat((double)((py + r + b - (T)1) / b))));
+  if (rmax[0] < rmin[0]) rmax[0] = rmin[0];
+  if (rmax[0] - rmin[0] > gx) rmax[0] = rmin[0] + gx;
+}
+
+template <class T>
+inline void tile_rect(bool seam_wrap, T px, T py, int max_radius, int gx, int gy, int rmin[2], int rmax[2]) {
+  if (seam_wrap)
+    get_rect_cyclic<T>(px, py, max_radius, gx, gy, rmin, rmax);
+  else
+    get_rect<T>(px, py, max_radius, gx, gy, rmin, rmax);
+}
+
+// x offset of a splat centre from a pixel column: the plain difference (the reference), or in
+// seam-wrapping mode the difference to the centre's copy (shifted by a multiple of the image
+// width) nearest the pixel.
+inline double seam_dx(bool seam_wrap, double mx, double px, int W) {
+  if (seam_wrap) mx -= W * std::nearbyint((mx - px) / W);
+  return mx - px;
+}
+
 // getHigherMsb, rasterizer_impl.cu:47-62.
 uint32_t higher_msb(uint32_t n) {
   uint32_t msb = sizeof(n) * 4;
@@ -255,13 +290,14 @@ uint32_t oracle_higher_msb(uint32_t n) { return higher_msb(n); }
 // Forward preprocess (forward.cu:592-703) in FP64.  Outputs: radii [P] (0 = culled), tiles_touched
 // [P], means2D [P,2] (pixels), depths [P] (radial distance r, forward.cu:697), conic_opacity [P,4],
 // rgb [P,3], clamped [P,3], cov3D [P,6].
-void oracle_preprocess(int P, int D, int M, int W, int H, const float* means3D, const float* scales,
-                       float scale_modifier, const float* rotations, const float* opacities,
-                       const float* shs, const float* colors_precomp, const float* cov3D_precomp,
-                       const float* viewmatrix, const float* campos, int* radii,
-                       uint32_t* tiles_touched, double* means2D, double* depths,
-                       double* conic_opacity, double* rgb, uint8_t* clamped, double* cov3D_out,
-                       int nthreads) {
+// seam_wrap selects the cyclic tile rect of the seam-wrapping mode (get_rect_cyclic).
+void oracle_preprocess_seam(int P, int D, int M, int W, int H, const float* means3D, const float* scales,
+                            float scale_modifier, const float* rotations, const float* opacities,
+                            const float* shs, const float* colors_precomp, const float* cov3D_precomp,
+                            const float* viewmatrix, const float* campos, int* radii,
+                            uint32_t* tiles_touched, double* means2D, double* depths,
+                            double* conic_opacity, double* rgb, uint8_t* clamped, double* cov3D_out,
+                            int seam_wrap, int nthreads) {
   const int gx = (W + kTile - 1) / kTile, gy = (H + kTile - 1) / kTile;
   const D3 cam = {campos[0], campos[1], campos[2]};
   parallel_for(P, nthreads, [&](int64_t i) {
@@ -296,7 +332,7 @@ void oracle_preprocess(int P, int D, int M, int W, int H, const float* means3D, 
     const double py = ((sy + 1.0) * H - 1.0) * 0.5;
     const int ir = to_int_sat(my_radius);
     int rmin[2], rmax[2];
-    get_rect<double>(px, py, ir, gx, gy, rmin, rmax);
+    tile_rect<double>(seam_wrap != 0, px, py, ir, gx, gy, rmin, rmax);
     const int64_t area = (int64_t)(rmax[0] - rmin[0]) * (rmax[1] - rmin[1]);
     if (area == 0) return;
     if (colors_precomp == nullptr) {
@@ -322,6 +358,18 @@ void oracle_preprocess(int P, int D, int M, int W, int H, const float* means3D, 
   });
 }
 
+void oracle_preprocess(int P, int D, int M, int W, int H, const float* means3D, const float* scales,
+                       float scale_modifier, const float* rotations, const float* opacities,
+                       const float* shs, const float* colors_precomp, const float* cov3D_precomp,
+                       const float* viewmatrix, const float* campos, int* radii,
+                       uint32_t* tiles_touched, double* means2D, double* depths,
+                       double* conic_opacity, double* rgb, uint8_t* clamped, double* cov3D_out,
+                       int nthreads) {
+  oracle_preprocess_seam(P, D, M, W, H, means3D, scales, scale_modifier, rotations, opacities, shs,
+                         colors_precomp, cov3D_precomp, viewmatrix, campos, radii, tiles_touched, means2D,
+                         depths, conic_opacity, rgb, clamped, cov3D_out, 0, nthreads);
+}
+
 // Total instances = inclusive scan's last element (rasterizer_impl.cu:622-628).
 int64_t oracle_num_rendered(int P, const uint32_t* tiles_touched) {
   int64_t s = 0;
@@ -335,7 +383,7 @@ namespace {
 template <class T>
 void binning_impl(int P, int W, int H, const int* radii, const T* means2D, const float* depth32,
                   const uint32_t* tiles_touched, uint64_t* keys_out, uint32_t* vals_out,
-                  uint32_t* ranges) {
+                  uint32_t* ranges, bool seam_wrap) {
   const int gx = (W + kTile - 1) / kTile, gy = (H + kTile - 1) / kTile;
   const int64_t tiles = (int64_t)gx * gy;
   std::vector<uint64_t> offs(P + 1, 0);
@@ -347,13 +395,14 @@ void binning_impl(int P, int W, int H, const int* radii, const T* means2D, const
   for (int i = 0; i < P; ++i) {
     if (!(radii[i] > 0)) continue;
     int rmin[2], rmax[2];
-    get_rect<T>(means2D[2 * i], means2D[2 * i + 1], radii[i], gx, gy, rmin, rmax);
+    tile_rect<T>(seam_wrap, means2D[2 * i], means2D[2 * i + 1], radii[i], gx, gy, rmin, rmax);
     uint64_t off = offs[i];
     uint32_t dbits;
     std::memcpy(&dbits, &depth32[i], 4);
     for (int y = rmin[1]; y < rmax[1]; ++y)
       for (int x = rmin[0]; x < rmax[0]; ++x) {
-        uint64_t key = (uint32_t)(y * gx + x);
+        const int col = ((x % gx) + gx) % gx;  // x itself unless the seam wraps
+        uint64_t key = (uint32_t)(y * gx + col);
         key <<= 32;
         key |= dbits;
         keys[off] = key;
@@ -401,23 +450,52 @@ extern "C" {
 void oracle_binning_f32(int P, int W, int H, const int* radii, const float* means2D,
                         const float* depths, const uint32_t* tiles_touched, uint64_t* keys,
                         uint32_t* vals, uint32_t* ranges) {
-  binning_impl<float>(P, W, H, radii, means2D, depths, tiles_touched, keys, vals, ranges);
+  binning_impl<float>(P, W, H, radii, means2D, depths, tiles_touched, keys, vals, ranges, false);
 }
 
-// Binning from the FP64 preprocess (rects in double; the key's depth bits are float(r)).
+// Tiles touched per Gaussian from its float rect (clamped, or cyclic when seam_wrap != 0): the
+// preprocess's tiles_touched for callers that hold only radii and means2D.
+void oracle_tiles_touched_f32(int P, int W, int H, const int* radii, const float* means2D, int seam_wrap,
+                              uint32_t* tiles_touched) {
+  const int gx = (W + kTile - 1) / kTile, gy = (H + kTile - 1) / kTile;
+  for (int i = 0; i < P; ++i) {
+    tiles_touched[i] = 0;
+    if (!(radii[i] > 0)) continue;
+    int rmin[2], rmax[2];
+    tile_rect<float>(seam_wrap != 0, means2D[2 * i], means2D[2 * i + 1], radii[i], gx, gy, rmin, rmax);
+    tiles_touched[i] = (uint32_t)((rmax[0] - rmin[0]) * (rmax[1] - rmin[1]));
+  }
+}
+
+// The same with the seam-wrapping mode's cyclic rects (seam_wrap != 0).
+void oracle_binning_f32_seam(int P, int W, int H, const int* radii, const float* means2D,
+                             const float* depths, const uint32_t* tiles_touched, uint64_t* keys,
+                             uint32_t* vals, uint32_t* ranges, int seam_wrap) {
+  binning_impl<float>(P, W, H, radii, means2D, depths, tiles_touched, keys, vals, ranges, seam_wrap != 0);
+}
+
+// Binning from the FP64 preprocess (rects in double; the key's depth bits are float(r)),
+// seam_wrap != 0 for the seam-wrapping mode's cyclic rects.
+void oracle_binning_f64_seam(int P, int W, int H, const int* radii, const double* means2D,
+                             const double* depths, const uint32_t* tiles_touched, uint64_t* keys,
+                             uint32_t* vals, uint32_t* ranges, int seam_wrap) {
+  std::vector<float> d32(P);
+  for (int i = 0; i < P; ++i) d32[i] = (float)depths[i];
+  binning_impl<double>(P, W, H, radii, means2D, d32.data(), tiles_touched, keys, vals, ranges, seam_wrap != 0);
+}
+
 void oracle_binning_f64(int P, int W, int H, const int* radii, const double* means2D,
                         const double* depths, const uint32_t* tiles_touched, uint64_t* keys,
                         uint32_t* vals, uint32_t* ranges) {
-  std::vector<float> d32(P);
-  for (int i = 0; i < P; ++i) d32[i] = (float)depths[i];
-  binning_impl<double>(P, W, H, radii, means2D, d32.data(), tiles_touched, keys, vals, ranges);
+  oracle_binning_f64_seam(P, W, H, radii, means2D, depths, tiles_touched, keys, vals, ranges, 0);
 }
 
 // Forward blend, forward.cu:346-467.  out_color [3,H,W], final_T [H*W], n_contrib [H*W].
-void oracle_render_forward(int W, int H, const uint32_t* ranges, const uint32_t* point_list,
-                           const double* means2D, const double* conic_opacity, const double* rgb,
-                           const float* bg, double* out_color, double* final_T,
-                           uint32_t* n_contrib, int nthreads) {
+// seam_wrap != 0: x offsets to the splat's copy nearest the pixel (seam_dx).
+void oracle_render_forward_seam(int W, int H, const uint32_t* ranges, const uint32_t* point_list,
+                                const double* means2D, const double* conic_opacity, const double* rgb,
+                                const float* bg, double* out_color, double* final_T,
+                                uint32_t* n_contrib, int seam_wrap, int nthreads) {
   const int gx = (W + kTile - 1) / kTile, gy = (H + kTile - 1) / kTile;
   parallel_for((int64_t)gx * gy, nthreads, [&](int64_t tile) {
     const int tx = (int)(tile % gx), ty = (int)(tile / gx);
@@ -429,7 +507,7 @@ void oracle_render_forward(int W, int H, const uint32_t* ranges, const uint32_t*
         for (uint32_t s = r0; s < r1; ++s) {
           contributor++;
           const uint32_t g = point_list[s];
-          const double dx = means2D[2 * g] - px, dy = means2D[2 * g + 1] - py;
+          const double dx = seam_dx(seam_wrap != 0, means2D[2 * g], px, W), dy = means2D[2 * g + 1] - py;
           const double* co = conic_opacity + 4 * (int64_t)g;
           const double power = -0.5 * (co[0] * dx * dx + co[2] * dy * dy) - co[1] * dx * dy;
           if (power > 0.0) continue;
@@ -449,17 +527,27 @@ void oracle_render_forward(int W, int H, const uint32_t* ranges, const uint32_t*
   });
 }
 
+void oracle_render_forward(int W, int H, const uint32_t* ranges, const uint32_t* point_list,
+                           const double* means2D, const double* conic_opacity, const double* rgb,
+                           const float* bg, double* out_color, double* final_T,
+                           uint32_t* n_contrib, int nthreads) {
+  oracle_render_forward_seam(W, H, ranges, point_list, means2D, conic_opacity, rgb, bg, out_color, final_T,
+                             n_contrib, 0, nthreads);
+}
+
 // Backward blend, backward.cu:672-843.  Gradients are accumulated per sorted instance (each
 // instance belongs to one tile, so tiles run in parallel without races) and then summed per
 // Gaussian in instance order, which makes the oracle deterministic.
 // Outputs (zeroed here): dL_dmean2D [P,3], dL_dconic [P,4] (x, y, -, w), dL_dopacity [P],
 // dL_dcolor [P,3].
-void oracle_render_backward(int P, int W, int H, const uint32_t* ranges, const uint32_t* point_list,
-                            int64_t R, const double* means2D, const double* conic_opacity,
-                            const double* rgb, const float* bg, const double* final_T,
-                            const uint32_t* n_contrib, const float* dL_dpix, double* dL_dmean2D,
-                            double* dL_dconic, double* dL_dopacity, double* dL_dcolor,
-                            int nthreads) {
+// seam_wrap != 0: x offsets to the splat's copy nearest the pixel (seam_dx); the offset's
+// derivative with respect to the centre is 1 for every copy, so the formulas are unchanged.
+void oracle_render_backward_seam(int P, int W, int H, const uint32_t* ranges, const uint32_t* point_list,
+                                 int64_t R, const double* means2D, const double* conic_opacity,
+                                 const double* rgb, const float* bg, const double* final_T,
+                                 const uint32_t* n_contrib, const float* dL_dpix, double* dL_dmean2D,
+                                 double* dL_dconic, double* dL_dopacity, double* dL_dcolor,
+                                 int seam_wrap, int nthreads) {
   const int gx = (W + kTile - 1) / kTile, gy = (H + kTile - 1) / kTile;
   std::vector<double> inst((size_t)R * 9, 0.0);
   const double ddelx_dx = 0.5 * W, ddely_dy = 0.5 * H;
@@ -478,7 +566,7 @@ void oracle_render_backward(int P, int W, int H, const uint32_t* ranges, const u
         for (int64_t k = (int64_t)last - 1; k >= 0; --k) {
           const uint32_t s = r0 + (uint32_t)k;
           const uint32_t g = point_list[s];
-          const double dx = means2D[2 * g] - px, dy = means2D[2 * g + 1] - py;
+          const double dx = seam_dx(seam_wrap != 0, means2D[2 * g], px, W), dy = means2D[2 * g + 1] - py;
           const double* co = conic_opacity + 4 * (int64_t)g;
           const double power = -0.5 * (co[0] * dx * dx + co[2] * dy * dy) - co[1] * dx * dy;
           if (power > 0.0) continue;
@@ -527,6 +615,16 @@ void oracle_render_backward(int P, int W, int H, const uint32_t* ranges, const u
     dL_dopacity[g] += a[5];
     for (int ch = 0; ch < 3; ++ch) dL_dcolor[3 * (int64_t)g + ch] += a[6 + ch];
   }
+}
+
+void oracle_render_backward(int P, int W, int H, const uint32_t* ranges, const uint32_t* point_list,
+                            int64_t R, const double* means2D, const double* conic_opacity,
+                            const double* rgb, const float* bg, const double* final_T,
+                            const uint32_t* n_contrib, const float* dL_dpix, double* dL_dmean2D,
+                            double* dL_dconic, double* dL_dopacity, double* dL_dcolor,
+                            int nthreads) {
+  oracle_render_backward_seam(P, W, H, ranges, point_list, R, means2D, conic_opacity, rgb, bg, final_T, n_contrib,
+                              dL_dpix, dL_dmean2D, dL_dconic, dL_dopacity, dL_dcolor, 0, nthreads);
 }
 
 // Backward preprocess: computeCov2DLonLatCUDA (backward.cu:297-485) + preprocessLonLatCUDA

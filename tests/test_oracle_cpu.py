@@ -3,7 +3,8 @@ semantics, and an FP64 central finite-difference check of its backward.
 
 The reference ships no tests or golden vectors, so these cases are built from first principles
 (cuda_rasterizer/auxiliary.h:51-66, 198-248 and forward.cu:130-189, 592-703); the oracle is
-additionally pinned to the reference's own outputs in test_oracle_golden.py.
+additionally pinned to the reference's own outputs, stage by stage, in
+test_oracle_vs_reference_gpu.py.
 """
 import math
 
@@ -181,3 +182,110 @@ def test_backward_matches_fp64_central_differences(seed):
     # inputs are float32, so perturbations are float32-rounded; compare robustly
     assert np.median(errs) < 1e-3, np.percentile(errs, [50, 90, 99])
     assert np.percentile(errs, 90) < 2e-2, np.percentile(errs, [50, 90, 99])
+
+
+# ---------------------------------------------------------------- seam-wrapping mode ----------
+def _yaw90_view(W, H):
+    """Camera turned by exactly 90 degrees of yaw about +y (integer rotation matrix, so the view
+    matrix is exact in float32): every longitude decreases by pi / 2, i.e. W / 4 pixels."""
+    R_wc = np.array([[0.0, 0.0, 1.0], [0.0, 1.0, 0.0], [-1.0, 0.0, 0.0]])
+    return scenes.make_view(W, H, (0.0, 0.0, 0.0), R_wc)
+
+
+def test_seam_wrap_known_answer_single_splat():
+    """A splat centred half a pixel left of the right image edge (longitude just below +pi): with
+    seam wrapping its tile rect continues in column 0 and it colours pixels of column 0; with the
+    reference's clamped rects it does not."""
+    W, H = 256, 128
+    g = scenes.make_gaussians(1, seed=0)
+    lon = math.pi - math.pi / W  # half a pixel left of the seam: px = W - 1
+    g.means3D[0] = np.array([2.0 * math.sin(lon), 0.0, 2.0 * math.cos(lon)], np.float32)
+    g.scales[0] = 0.05
+    g.opacities[0] = 0.9
+    v = scenes.identity_view(W, H)
+    bg = np.zeros(3, np.float32)
+    for wrap in (False, True):
+        pre = oracle.preprocess(g.means3D, g.scales, g.rotations, g.opacities, g.shs, v.viewmatrix,
+                                v.campos, W, H, seam_wrap=wrap)
+        assert pre["radii"][0] > 0 and abs(pre["means2D"][0, 0] - (W - 1)) < 1.0
+        b = oracle.binning(W, H, pre["radii"], pre["means2D"], pre["depths"], pre["tiles_touched"],
+                           f32=False, seam_wrap=wrap)
+        cols = set(int(k >> 32) % (W // 16) for k in b["keys"])
+        fw = oracle.render_forward(W, H, b["ranges"], b["point_list"], pre["means2D"],
+                                   pre["conic_opacity"], pre["rgb"], bg, seam_wrap=wrap)
+        col0 = float(1.0 - fw["final_T"].reshape(H, W)[:, 0].min())
+        if wrap:
+            assert 0 in cols and W // 16 - 1 in cols
+            assert col0 > 0.1  # the splat's wrapped half
+        else:
+            assert 0 not in cols
+            assert col0 == 0.0
+
+
+@pytest.mark.parametrize("wrap", [False, True])
+def test_seam_wrap_yaw_by_a_quarter_turn_rolls_the_image(wrap):
+    """Turning the camera by exactly 90 degrees of yaw rolls the equirect image by W / 4 pixels (a
+    whole number of tiles).  With seam wrapping this holds to FP64 rounding everywhere, including
+    the splats that straddle the seam, and the gradients with respect to the Gaussians are
+    unchanged; with the reference's clamped rects the columns at the two seams differ."""
+    W, H = 256, 128
+    g = scenes.make_gaussians(3000, seed=31, seam_fraction=0.4)
+    dpix = scenes.upstream_grad(W, H, seed=31)
+    a = oracle.forward_backward(g, scenes.identity_view(W, H), dpix, seam_wrap=wrap)
+    b = oracle.forward_backward(g, _yaw90_view(W, H), np.roll(dpix, -W // 4, axis=2), seam_wrap=wrap)
+    rolled = np.roll(a["image"], -W // 4, axis=2)
+    diff = np.abs(b["image"] - rolled)
+    seam_cols = np.zeros(W, bool)
+    for c in (W - W // 4, 0):  # image a's seam after the roll, image b's own seam
+        for d in range(-16, 16):
+            seam_cols[(c + d) % W] = True
+    if wrap:
+        assert diff.max() < 1e-9, diff.max()
+        for name in ("dL_dmeans3D", "dL_dsh", "dL_dopacity", "dL_dscales", "dL_drotations"):
+            ga, gb = a[name], b[name]
+            assert np.abs(ga - gb).max() <= 1e-9 * max(np.abs(ga).max(), 1e-30), name
+    else:
+        assert diff[:, :, ~seam_cols].max() < 1e-9
+        assert diff[:, :, seam_cols].max() > 1e-2
+
+
+def test_seam_wrap_backward_matches_fp64_central_differences():
+    """FP64 central differences of L = <dL/dpix, image> against the oracle's backward in seam
+    wrapping mode, on splats straddling the seam (x offsets to the nearest copy)."""
+    Wf, Hf = 128, 64
+    rng = np.random.default_rng(3)
+    g = scenes.make_gaussians(40, seed=13, seam_fraction=1.0, seam_width_deg=6.0)
+    g.scales[:] = np.exp(rng.normal(np.log(0.06), 0.2, g.scales.shape)).astype(np.float32)
+    v = scenes.identity_view(Wf, Hf)
+    dpix = scenes.upstream_grad(Wf, Hf, seed=3)
+
+    def loss(gs):
+        out = oracle.forward_backward(gs, v, dpix, nthreads=1, seam_wrap=True)
+        return float((out["image"] * dpix).sum()), out
+
+    _, out = loss(g)
+    vis = np.nonzero(out["pre"]["radii"] > 0)[0]
+    assert len(vis) > 10
+    # some splats really do straddle: their rects wrap
+    assert (out["pre"]["tiles_touched"] > 0).sum() == len(vis)
+    errs = []
+    for field, gname, eps in (("means3D", "dL_dmeans3D", 1e-4), ("opacities", "dL_dopacity", 1e-5),
+                              ("shs", "dL_dsh", 1e-4), ("scales", "dL_dscales", 1e-5)):
+        arr = getattr(g, field)
+        flat = arr.reshape(arr.shape[0], -1)
+        ana_all = out[gname].reshape(arr.shape[0], -1)
+        for i in vis[:10]:
+            for k in range(min(flat.shape[1], 3)):
+                orig = flat[i, k]
+                flat[i, k] = orig + eps
+                hi = float(flat[i, k])
+                lp, _ = loss(g)
+                flat[i, k] = orig - eps
+                lo = float(flat[i, k])
+                lm, _ = loss(g)
+                flat[i, k] = orig
+                fd = (lp - lm) / (hi - lo)
+                ana = ana_all[i, k]
+                errs.append(abs(fd - ana) / max(abs(fd), abs(ana), 1e-3 * np.abs(ana_all).max()))
+    errs = np.array(errs)
+    assert errs.max() < 1e-4, np.percentile(errs, [50, 90, 99])
