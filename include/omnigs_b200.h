@@ -146,8 +146,13 @@ int omnigs_lonlat_forward(const OmnigsLonlatForwardArgs* args, void* geom, size_
  * W * H <= 262144 and the instances must fit the rest of the array (OMNIGS_ERR_CAPACITY
  * otherwise).  It allocates no device memory; it waits for `stream` at the end to read the status
  * and returns num_rendered.  The first call on a device looks up the array's device address
- * (cudaGetSymbolAddress); make that first call before any stream capture.  All calls share the
- * array: calls that overlap on the GPU race and must not be issued. */
+ * (cudaGetSymbolAddress); make that first call before any stream capture.  Under CUDA's default
+ * lazy module loading the array is reserved when this library's kernels are first used on a
+ * device, which can be that first call; a caller that then reserves all remaining device memory
+ * should make one early call first (P = 0 suffices) or run with CUDA_MODULE_LOADING=EAGER.  The
+ * looked-up address is kept for the life of the process: do not use this entry point on a device
+ * after cudaDeviceReset.  All calls share the array: calls that overlap on the GPU race and must
+ * not be issued. */
 int omnigs_lonlat_forward_noalloc(const OmnigsLonlatForwardArgs* args, int* num_rendered,
                                   omnigs_stream_t stream);
 
@@ -292,6 +297,17 @@ int omnigs_batch_autotune(const OmnigsBatchArgs* args, void* state, size_t state
 int omnigs_batch_read_status(const void* state, int V, int64_t* num_rendered, int64_t* view_rendered,
                              uint32_t* status, omnigs_stream_t stream);
 
+/* Failure-path check of the bounded cross-block waits (no counterpart in the reference): runs
+ * omnigs_lonlat_preprocess and the binning up to the duplicate pass with scan tile 0 taken by no
+ * block, so tile 1's look-back waits on a prefix that is never published; the wait gives up after
+ * max_spins polls, sets OMNIGS_STATUS_LOOKBACK and the kernel finishes.  Then waits for `stream`,
+ * returns the status word in *status and OMNIGS_ERR_DEVICE when a bit other than capacity is set.
+ * The buffers hold no valid forward afterwards; a following omnigs_lonlat_forward resets them.
+ * Needs P > 256.  For tests: real passes never skip a tile. */
+int omnigs_debug_lookback_timeout(const OmnigsLonlatForwardArgs* args, void* geom, size_t geom_bytes,
+                                  void* binning, size_t binning_bytes, void* image, size_t image_bytes,
+                                  int max_spins, uint32_t* status, omnigs_stream_t stream);
+
 /* Device pointers into the batch state, for inspection and parity testing.  Pixels of view v start
  * at pixel_base[v] of final_T / n_contrib, its tiles at tile_base[v] of ranges. */
 typedef struct OmnigsBatchStateView {
@@ -304,6 +320,7 @@ typedef struct OmnigsBatchStateView {
   int64_t pixel_base[OMNIGS_MAX_BATCH_VIEWS];
   int64_t tile_base[OMNIGS_MAX_BATCH_VIEWS];
   int tile_passes;              /* tile-sort passes: the sorted list is in buffer (tile_passes & 1) */
+  const float* depth;           /* [V][P] radial distance (the sort key's depth bits) */
 } OmnigsBatchStateView;
 int omnigs_batch_state_view(const void* state, int P, int V, const int* W, const int* H,
                             OmnigsBatchStateView* out);
@@ -408,7 +425,7 @@ uint64_t omnigs_kernel_launches(void);
 /* Read-only views into the private buffers, for inspection and parity testing.  Pointers are
  * device pointers inside the given buffers. */
 typedef struct OmnigsLonlatGeomView {
-  const float* splat;          /* [P][8]: x, y, conic a, conic b, conic c, opacity, cull hx, cull hy */
+  const float* splat;          /* [P][8]: x, y, conic a, conic b, conic c, opacity, cull threshold, conic det */
   const float* color;          /* [P][4]: r, g, b, clamp bits (as uint32) */
   const float* depth;          /* [P] radial distance r (+inf where culled) */
   const uint32_t* tiles_touched; /* [P] */
@@ -429,6 +446,11 @@ int omnigs_lonlat_geom_view(const void* geom, int P, OmnigsLonlatGeomView* out);
 int omnigs_lonlat_binning_view(const void* binning, size_t binning_bytes, int W, int H,
                                OmnigsLonlatBinningView* out);
 int omnigs_lonlat_image_view(const void* image, int W, int H, OmnigsLonlatImageView* out);
+/* The batch's sorted instance list in its binning buffer, after a forward: instance i covers global
+ * tile tile_ids[i] (view v owns tiles [tile_base[v], tile_base[v] + its tiles)) and splat record
+ * point_list[i] = v * P + Gaussian index.  No counterpart in the reference (inspection). */
+int omnigs_batch_binning_view(const void* binning, size_t binning_bytes, int P, int V, const int* W,
+                              const int* H, OmnigsLonlatBinningView* out);
 
 #ifdef __cplusplus
 }

@@ -94,7 +94,7 @@ class BatchStateView(ctypes.Structure):
     _fields_ = [("radii", _vp), ("splat", _vp), ("color", _vp), ("final_T", _vp),
                 ("n_contrib", _vp), ("ranges", _vp),
                 ("pixel_base", ctypes.c_int64 * MAX_BATCH_VIEWS),
-                ("tile_base", ctypes.c_int64 * MAX_BATCH_VIEWS), ("tile_passes", _i)]
+                ("tile_base", ctypes.c_int64 * MAX_BATCH_VIEWS), ("tile_passes", _i), ("depth", _vp)]
 
 
 class GaussianParams(ctypes.Structure):
@@ -133,9 +133,9 @@ EXPORTED = ["omnigs_version", "omnigs_last_error", "omnigs_lonlat_geom_bytes",
             "omnigs_kernel_launches", "omnigs_lonlat_geom_view", "omnigs_lonlat_binning_view",
             "omnigs_lonlat_image_view", "omnigs_batch_state_bytes", "omnigs_batch_forward",
             "omnigs_batch_render", "omnigs_batch_backward", "omnigs_batch_read_status",
-            "omnigs_batch_state_view", "omnigs_l1_dssim_workspace_bytes", "omnigs_l1_dssim",
+            "omnigs_batch_state_view", "omnigs_batch_binning_view", "omnigs_l1_dssim_workspace_bytes", "omnigs_l1_dssim",
             "omnigs_activate", "omnigs_adam_step", "omnigs_set_blend_batch", "omnigs_get_blend_batch",
-            "omnigs_batch_autotune"]
+            "omnigs_batch_autotune", "omnigs_debug_lookback_timeout"]
 
 _lib = None
 
@@ -189,6 +189,9 @@ def lib() -> ctypes.CDLL:
                                                ctypes.POINTER(ctypes.c_int64),
                                                ctypes.POINTER(ctypes.c_uint32), _vp]
         L.omnigs_batch_state_view.argtypes = [_vp, _i, _i, ip, ip, ctypes.POINTER(BatchStateView)]
+        L.omnigs_debug_lookback_timeout.argtypes = fw + [_vp, ctypes.c_size_t, _vp, ctypes.c_size_t, _i,
+                                                         ctypes.POINTER(ctypes.c_uint32), _vp]
+        L.omnigs_batch_binning_view.argtypes = [_vp, ctypes.c_size_t, _i, _i, ip, ip, ctypes.POINTER(BinningView)]
         L.omnigs_l1_dssim_workspace_bytes.restype = ctypes.c_size_t
         L.omnigs_l1_dssim_workspace_bytes.argtypes = [_i, _i, _i]
         L.omnigs_l1_dssim.argtypes = [_vp, _vp, _i, _i, _i, _i, _f, _vp, _vp, _vp, ctypes.c_size_t, _vp]

@@ -354,7 +354,7 @@ __global__ void __launch_bounds__(kScanBlock) duplicate_kernel(const __grid_cons
     return;
   }
   if (kPerView && blockIdx.x == 0 && threadIdx.x < p.V) p.key_base_out[threadIdx.x] = p.tile_base[threadIdx.x];
-  if (threadIdx.x == 0) s_tile = atomicAdd(&p.hdr->dup_tile_counter, 1u);
+  if (threadIdx.x == 0) s_tile = atomicAdd(&p.hdr->dup_tile_counter, 1u) + p.skip_tiles;
   for (int k = threadIdx.x; k < kSlots * kHistSlot; k += kScanBlock) s_hist[k] = 0;
   __syncthreads();
   const uint32_t tile = s_tile;
@@ -421,6 +421,7 @@ __global__ void __launch_bounds__(kScanBlock) duplicate_kernel(const __grid_cons
       unsigned long long excl = 0;
       long long base = (long long)tile - 1;
       bool gave_up = false;
+      const int max_spins = p.max_spins > 0 ? p.max_spins : kMaxSpins;
       for (;;) {
         const long long j = base - lane;
         unsigned long long w = kScanPrefix;  // virtual zero prefix before the first block
@@ -428,7 +429,7 @@ __global__ void __launch_bounds__(kScanBlock) duplicate_kernel(const __grid_cons
           w = ld_relaxed_u64(&p.scan_state[j]);
           int spins = 0;
           while ((w >> 62) == 0) {
-            if (++spins > kMaxSpins) {
+            if (++spins > max_spins) {
               gave_up = true;
               w = kScanPrefix;
               break;
@@ -501,13 +502,17 @@ __global__ void __launch_bounds__(kScanBlock) duplicate_kernel(const __grid_cons
       p.tvals[o] = o_g;
     }
     // digit histograms of the tile sort (the pass that would otherwise re-read every key)
-    const unsigned live = __ballot_sync(kFullMask, ok);
     const uint32_t slot = kPerView ? __shfl_sync(kFullMask, my_view, pos) - view0 : 0u;
+    // A block spans at most kSlots views when every view has at least kScanBlock Gaussians (the
+    // batched entry points require that); a slot past them is counted nowhere and flagged.
+    const bool counted = ok && slot < (uint32_t)kSlots;
+    if (kPerView && __any_sync(kFullMask, ok && !counted) && lane == 0) atomicOr(&p.hdr->status, kStatusInconsistent);
+    const unsigned live = __ballot_sync(kFullMask, counted);
 #pragma unroll
     for (int q = 0; q < kTilePasses; ++q)
       if (q < p.hist_passes)
-        count_digit(s_hist, slot * kHistSlot + q * kRadix + ((key >> p.hist_shift[q]) & p.hist_mask[q]), ok, live,
-                    lane);
+        count_digit(s_hist, slot * kHistSlot + q * kRadix + ((key >> p.hist_shift[q]) & p.hist_mask[q]), counted,
+                    live, lane);
   }
   if (p.hist_passes == 0) return;
   __syncthreads();
@@ -573,7 +578,10 @@ void launch_onesweep(const OnesweepParams& p, int64_t max_items, cudaStream_t s)
 void launch_duplicate(const DuplicateParams& p, cudaStream_t s) {
   const int64_t items = (int64_t)p.P * p.V;
   if (items <= 0) return;
-  const unsigned blocks = (unsigned)((items + kScanBlock - 1) / kScanBlock);
+  const int64_t tiles = (items + kScanBlock - 1) / kScanBlock;
+  if (tiles <= (int64_t)p.skip_tiles) return;
+  // one block per scan tile that is taken: block k takes tile skip_tiles + k
+  const unsigned blocks = (unsigned)(tiles - p.skip_tiles);
   if (p.hist_per_view)
     duplicate_kernel<true><<<blocks, kScanBlock, 0, s>>>(p);
   else

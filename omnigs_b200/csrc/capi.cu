@@ -218,12 +218,18 @@ EarlyStatus* early_status_slot() {
   return &e;
 }
 
+// A forward cut short after the duplicate pass, whose scan tile 0 is taken by no block and whose
+// look-back waits give up after max_spins polls (omnigs_debug_lookback_timeout).
+struct LookbackProbe {
+  int max_spins;
+};
+
 // Binning + forward blend.  With `early`, the header (instance count, status word; final once the
 // binning kernels have run) is copied to early->host and early->copied recorded between the binning
-// and the blend.
+// and the blend.  With `probe`, the pass stops after the duplicate kernel (see LookbackProbe).
 int render_impl(const OmnigsLonlatForwardArgs* a, void* geom, size_t geom_bytes, void* binning,
                 size_t binning_bytes, void* image, size_t image_bytes, omnigs_stream_t stream,
-                EarlyStatus* early) {
+                EarlyStatus* early, const LookbackProbe* probe = nullptr) {
   if (int rc = validate_forward(a)) return rc;
   cudaStream_t s = reinterpret_cast<cudaStream_t>(stream);
   const int64_t HW = (int64_t)a->W * a->H;
@@ -315,7 +321,12 @@ int render_impl(const OmnigsLonlatForwardArgs* a, void* geom, size_t geom_bytes,
     d.hist_shift[q] = td.shift[q];
     d.hist_mask[q] = td.mask[q];
   }
+  if (probe != nullptr) {
+    d.max_spins = probe->max_spins;
+    d.skip_tiles = 1;
+  }
   staged(OMNIGS_STAGE_DUPLICATE, 1, s, [&] { launch_duplicate(d, s); });
+  if (probe != nullptr) return check_launch("duplicate (look-back probe)");
 
   // 3. stable tile sort of the instances
   // (its digit histograms were counted by the duplicate pass)
@@ -407,6 +418,28 @@ int omnigs_lonlat_forward_early_status(const OmnigsLonlatForwardArgs* a, void* g
   const unsigned long long n = e->host->num_rendered64;
   *num_rendered = (int)(n > 0x7fffffffull ? 0x7fffffff : n);
   *status = e->host->status;
+  return OMNIGS_OK;
+}
+
+int omnigs_debug_lookback_timeout(const OmnigsLonlatForwardArgs* a, void* geom, size_t geom_bytes, void* binning,
+                                  size_t binning_bytes, void* image, size_t image_bytes, int max_spins,
+                                  uint32_t* status, omnigs_stream_t stream) {
+  g_last_error.clear();
+  if (a == nullptr || status == nullptr) return fail(OMNIGS_ERR_INVALID_ARGUMENT, "NULL argument");
+  if (max_spins <= 0) return fail(OMNIGS_ERR_INVALID_ARGUMENT, "max_spins must be positive");
+  if (a->P <= kScanBlock)
+    return fail(OMNIGS_ERR_INVALID_ARGUMENT, "the look-back probe needs more than one scan tile of Gaussians");
+  if (int rc = omnigs_lonlat_preprocess(a, geom, geom_bytes, stream)) return rc;
+  const LookbackProbe probe{max_spins};
+  if (int rc = render_impl(a, geom, geom_bytes, binning, binning_bytes, image, image_bytes, stream, nullptr, &probe))
+    return rc;
+  int n = 0;
+  if (int rc = omnigs_lonlat_read_status(geom, &n, status, stream)) return rc;
+  if (*status & ~OMNIGS_STATUS_CAPACITY) {
+    const std::string msg = "device status " + std::to_string(*status) +
+                            (*status & OMNIGS_STATUS_LOOKBACK ? ": a bounded look-back wait gave up" : "");
+    return fail(OMNIGS_ERR_DEVICE, msg.c_str());
+  }
   return OMNIGS_OK;
 }
 

@@ -101,6 +101,11 @@ struct DuplicateParams {
   uint32_t hist_mask[kTilePasses];
   int hist_per_view;
   uint32_t* key_base_out;      // with hist_per_view: tile_base[0, V) copied here for the tile sort
+  // Look-back wait limit (polls; 0 = kMaxSpins) and the number of leading scan tiles no block
+  // takes (0 in every real pass).  omnigs_debug_lookback_timeout sets skip_tiles = 1 and a small
+  // limit: tile 0 then never publishes its prefix, so tile 1's bounded wait runs out.
+  int max_spins;
+  uint32_t skip_tiles;
 };
 
 struct RangesParams {

@@ -59,3 +59,27 @@ def test_noalloc_forward_rejects_scenes_over_its_limits(cuda):
     cam = lonlat.Camera.from_view(scenes.identity_view(64, 32))
     with pytest.raises(capi.OmnigsError, match="exceeds the no-allocation limit"):
         _noalloc_forward(gt, cam)
+    small = lonlat.GaussianTensors.from_numpy(scenes.make_gaussians(1000, seed=22))
+    big_image = lonlat.Camera.from_view(scenes.identity_view(1024, 512))  # above 512 x 512 pixels
+    with pytest.raises(capi.OmnigsError, match="exceeds the no-allocation limit"):
+        _noalloc_forward(small, big_image)
+
+
+def test_noalloc_forward_reports_instance_overflow_then_recovers(cuda):
+    """Instances that overflow the rest of the array are detected on the device and reported as a
+    capacity error; the next call starts from a clean state (the array keeps the failed call's
+    contents, and the forward clears its header first) and matches the allocating forward."""
+    W, H = 512, 512
+    g = scenes.make_gaussians(32_768, seed=23)
+    g.scales *= 12.0  # large splats: ~30 tiles each, far more instances than the array holds
+    big = lonlat.GaussianTensors.from_numpy(g)
+    cam = lonlat.Camera.from_view(scenes.identity_view(W, H))
+    with pytest.raises(capi.OmnigsError, match="instances exceed"):
+        _noalloc_forward(big, cam)
+    small = lonlat.GaussianTensors.from_numpy(scenes.make_gaussians(10_000, seed=24))
+    img, radii, n, _ = lonlat.rasterize(small, cam)
+    img2, radii2, n2 = _noalloc_forward(small, cam)
+    torch.cuda.synchronize()
+    assert n2 == n
+    assert torch.equal(radii2, radii)
+    assert float((img2 - img).abs().max()) <= IMG_ATOL
