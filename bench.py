@@ -24,8 +24,14 @@ across ranks every step with one NCCL all-reduce, as a data-parallel train step 
   peak) over the measured step time.
 * cpu_baseline: the FP64 oracle (multithreaded C++ restatement of the reference algorithm) on the
   same view, on this host's cores.
+* configs: the precision configuration (6M pole-heavy Gaussians, 4096x2048), peak memory at
+  4096x2048 over 3M Gaussians, and the differentiation configuration (500 Adam steps over 24 views
+  through the LibTorch autograd Function).
 * --impl reference: the reference arm.  The reference's rasterizer is CUDA-only, so its CPU
-  implementation of the path is the FP64 oracle port, timed here on all host cores.
+  implementation of the path is the FP64 oracle port, timed here on all host cores.  The same line
+  carries reference_gpu: the reference's own CUDA rasterizer rebuilt for sm_100a
+  (oracle/ref/Makefile), timed on this workload on the same GPU, and its peak memory at the
+  peak-memory workload -- the like-for-like GPU comparison.
 """
 from __future__ import annotations
 
@@ -59,7 +65,10 @@ def parse():
     ap.add_argument("--no-cpu-baseline", action="store_true")
     ap.add_argument("--no-e2e", action="store_true")
     ap.add_argument("--no-batch", action="store_true", help="skip the batched multi-view leg")
-    ap.add_argument("--no-extra", action="store_true", help="skip the precision and peak-memory legs")
+    ap.add_argument("--no-extra", action="store_true",
+                    help="skip the precision, peak-memory and differentiation legs")
+    ap.add_argument("--no-reference-gpu", action="store_true",
+                    help="skip the rebuilt reference rasterizer's GPU timing and peak memory")
     # smaller cases for profiling captures only; bench lines use the defaults
     ap.add_argument("--gaussians", type=int, default=P_GAUSS)
     ap.add_argument("--width", type=int, default=WIDTH)
@@ -283,6 +292,8 @@ def run_reference(args, rank, world):
                              "sample": f"{steps} full view(s); the reference rasterizer has no CPU "
                                        "path, so this is the FP64 oracle restating its algorithm"},
             "e2e": {"value": value, "unit": UNIT, "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0}}
+    if not args.no_reference_gpu:
+        line["reference_gpu"] = run_reference_gpu(args)
     print(json.dumps(line), flush=True)
 
 
@@ -487,6 +498,188 @@ def run_peak_memory(dev):
     del state, grads, img, gt
     torch.cuda.empty_cache()
     return out
+
+
+def run_differentiation(args, dev):
+    """Differentiation configuration: a perturbed copy of a 500k-Gaussian scene (means + N(0, 0.02 m),
+    SH + N(0, 0.1)) optimised for 500 Adam steps on L1 + 0.2 D-SSIM towards 24 target views at
+    2048x1024 (camera positions uniform in a 2 m cube, random yaw), one view per step in a seeded
+    random order per pass over the views, as the reference's trainer picks keyframes
+    (src/gaussian_mapper.cpp:384-432).  Each step runs through the LibTorch autograd Function:
+    GaussianRasterizer forward, the fused L1 + D-SSIM kernel for dL/dimage, image.backward() (the
+    C++ Function's backward, RasterizeGaussiansBackwardCUDA), fused Adam on the activated-value
+    gradients.  The targets are rendered from the unperturbed scene by the same rasterizer."""
+    import torch
+
+    from omnigs_b200 import GaussianRasterizationSettings, GaussianRasterizer, lonlat, scenes, train
+
+    P, W, H, V, STEPS = 500_000, 2048, 1024, 24, 500
+    gt_scene = scenes.make_gaussians(P, seed=6)
+    views = scenes.random_views(V, [(W, H)], seed=7, cube=2.0, pitch_deg=0.0)
+    cams = [lonlat.Camera.from_view(v, dev) for v in views]
+    gtt = lonlat.GaussianTensors.from_numpy(gt_scene, dev)
+    targets = []
+    for c in cams:
+        img, _, _, st = lonlat.rasterize(gtt, c)
+        targets.append(img.clone())
+        del st
+    del gtt
+    rng = np.random.Generator(np.random.PCG64(8))
+    pert = scenes.Gaussians(
+        (gt_scene.means3D + rng.normal(0.0, 0.02, gt_scene.means3D.shape)).astype(np.float32),
+        gt_scene.scales.copy(), gt_scene.rotations.copy(), gt_scene.opacities.copy(),
+        (gt_scene.shs + rng.normal(0.0, 0.1, gt_scene.shs.shape)).astype(np.float32))
+    model = train.GaussianModelState.from_activated(pert, device=dev)
+    settings = [GaussianRasterizationSettings(H, W, 0.0, 0.0, c.background, 1.0, c.viewmatrix, c.viewmatrix, 3,
+                                              c.campos) for c in cams]
+    order = np.concatenate([rng.permutation(V) for _ in range((STEPS + V - 1) // V)])[:STEPS]
+    losses = torch.zeros(STEPS, 3, device=dev)
+    loss_ws = train.l1_dssim_workspace(3, H, W, dev)
+
+    def render(i, leaves):
+        return GaussianRasterizer(settings[i])(leaves[0], leaves[1], leaves[2], shs=leaves[3], scales=leaves[4],
+                                               rotations=leaves[5])[0]
+
+    def psnr_all():
+        t = model.tensors()
+        vals = []
+        with torch.no_grad():
+            for i in range(V):
+                img = render(i, (t.means3D, torch.zeros_like(t.means3D), t.opacities, t.shs, t.scales,
+                                 t.rotations))
+                mse = float(((img - targets[i]) ** 2).mean())
+                vals.append(10.0 * math.log10(1.0 / max(mse, 1e-20)))
+        return round(statistics.mean(vals), 3)
+
+    psnr0 = psnr_all()
+    torch.cuda.synchronize()
+    e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+    t0 = time.perf_counter()
+    e0.record()
+    for k in range(STEPS):
+        i = int(order[k])
+        t = model.tensors()
+        leaves = [t.means3D.detach().requires_grad_(True), torch.zeros_like(t.means3D, requires_grad=True),
+                  t.opacities.detach().requires_grad_(True), t.shs.detach().requires_grad_(True),
+                  t.scales.detach().requires_grad_(True), t.rotations.detach().requires_grad_(True)]
+        img = render(i, leaves)
+        _, dimg = train.l1_dssim(img.detach(), targets[i], 0.2, loss=losses[k], workspace=loss_ws)
+        img.backward(dimg)
+        model.adam_step(leaves[0].grad, leaves[3].grad, leaves[2].grad, leaves[4].grad, leaves[5].grad)
+    e1.record()
+    torch.cuda.synchronize()
+    wall = time.perf_counter() - t0
+    ms = e0.elapsed_time(e1) / STEPS
+    psnr1 = psnr_all()
+    curve = losses[:, 0].cpu().numpy()
+    windows = {str(s): round(float(curve[max(0, s - V + 1):s + 1].mean()), 6)
+               for s in (V - 1, 49, 99, 199, 299, 399, STEPS - 1)}
+    out = {"workload": f"{P} Gaussians (perturbed copy: means + N(0,0.02), SH + N(0,0.1)), {V} target views "
+                       f"{W}x{H} from positions uniform in a 2 m cube with random yaw, {STEPS} Adam steps on "
+                       "L1 + 0.2 D-SSIM, one view per step, through the LibTorch autograd Function",
+           "ms_per_step": round(ms, 4), "wall_s": round(wall, 3), "steps": STEPS,
+           "loss_first": round(float(curve[0]), 6), "loss_last": round(float(curve[-1]), 6),
+           "loss_mean_of_last_24_views_at_step": windows,
+           "psnr_db_mean_over_views": {"before": psnr0, "after": psnr1},
+           "adam_step_count": model.step_count}
+    del model, targets
+    torch.cuda.empty_cache()
+    return out
+
+
+def run_reference_gpu(args):
+    """The reference's own CUDA rasterizer rebuilt for sm_100a from its sources (oracle/ref/Makefile)
+    on this arm's workload (1M Gaussians, one 2048x1024 view), device-timed like the main line with
+    its own clock record: forward + backward of one view per step (its forward copies num_rendered
+    to the host mid-pass, as its LibTorch layer does; gradient outputs zero-initialised as that
+    layer allocates them).  Plus its peak device memory at the peak-memory workload.  The
+    like-for-like GPU comparison; None where the library was not built (no reference checkout at
+    build time) or no GPU is visible."""
+    import torch
+
+    from omnigs_b200 import lonlat, scenes
+    from oracle import refcuda
+
+    if not (refcuda.available() and torch.cuda.is_available()):
+        return None
+    dev = torch.device("cuda", 0)
+    torch.cuda.set_device(dev)
+    g = scenes.make_gaussians(P_GAUSS, seed=0)
+    gt = lonlat.GaussianTensors.from_numpy(g, dev)
+    cam = lonlat.Camera.from_view(scenes.identity_view(WIDTH, HEIGHT), dev)
+    dpix = torch.from_numpy(scenes.upstream_grad(WIDTH, HEIGHT, seed=2)).to(dev)
+    gpu_uuid = None
+    try:
+        gpu_uuid = "GPU-" + str(torch.cuda.get_device_properties(dev).uuid)
+    except Exception:
+        pass
+    ref = refcuda.ReferenceRasterizer()
+    out = torch.zeros(3, cam.height, cam.width, device=dev)
+    radii = torch.zeros(g.P, dtype=torch.int32, device=dev)
+    n = [0]
+
+    def step():
+        _, r, n[0] = ref.forward(gt, cam, sync=False, out=out, radii=radii)
+        ref.backward(gt, cam, r, dpix, sync=False)
+
+    for _ in range(max(3, args.warmup)):
+        step()
+    torch.cuda.synchronize()
+    cur = torch.cuda.current_stream(dev)
+    e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+    with clock_sampler(gpu_uuid) as clocks:
+        e0.record(cur)
+        for _ in range(args.steps):
+            step()
+        e1.record(cur)
+        torch.cuda.synchronize()
+    ref.close()
+    ms = e0.elapsed_time(e1) / args.steps
+    del out, radii, gt, dpix
+    torch.cuda.empty_cache()
+    return {"impl": "reference CUDA rasterizer (cuda_rasterizer/, LonlatRasterizer::forward/backward) rebuilt "
+                    "for sm_100a", "workload": WORKLOAD, "ms_per_view": round(ms, 4),
+            "views_per_s": round(1000.0 / ms, 3), "steps": args.steps, "warmup": max(3, args.warmup),
+            "num_rendered": int(n[0]), "clocks": clocks.summary(),
+            "peak_memory": reference_peak_memory(dev)}
+
+
+def reference_peak_memory(dev):
+    """Peak device memory of one fwd+bwd of the rebuilt reference rasterizer at the peak-memory
+    workload: its state buffers (cudaMalloc'ed, measured as the drop in free device memory while
+    they are held) plus the output and gradient tensors its LibTorch layer would allocate."""
+    import torch
+
+    from omnigs_b200 import lonlat, scenes
+    from oracle import refcuda
+
+    if not refcuda.available():
+        return None
+    P, W, H = 3_000_000, 4096, 2048
+    g = scenes.make_gaussians(P, seed=3)
+    gt = lonlat.GaussianTensors.from_numpy(g, dev)
+    cam = lonlat.Camera.from_view(scenes.identity_view(W, H), dev)
+    dpix = torch.from_numpy(scenes.upstream_grad(W, H, seed=3)).to(dev)
+    torch.cuda.synchronize()
+    torch.cuda.empty_cache()
+    free0 = torch.cuda.mem_get_info(dev)[0]
+    reserved0 = torch.cuda.memory_reserved(dev)
+    base = torch.cuda.memory_allocated(dev)
+    torch.cuda.reset_peak_memory_stats(dev)
+    ref = refcuda.ReferenceRasterizer()
+    _, radii, n = ref.forward(gt, cam)
+    grads = ref.backward(gt, cam, radii, dpix)
+    torch.cuda.synchronize()
+    free1 = torch.cuda.mem_get_info(dev)[0]
+    torch_peak = torch.cuda.max_memory_allocated(dev) - base
+    state_bytes = (free0 - free1) - (torch.cuda.memory_reserved(dev) - reserved0)
+    ref.close()
+    del grads, radii, gt
+    torch.cuda.empty_cache()
+    peak = state_bytes + torch_peak
+    return {"num_rendered": int(n), "peak_bytes_above_inputs": int(peak), "peak_gb": round(peak / 1e9, 3),
+            "state_buffers_bytes": int(state_bytes), "per_pixel_state_bytes": 16 * W * H,
+            "method": "state buffers from the drop in free device memory + torch peak of outputs and gradients"}
 
 
 def _time_steps(fn, args, dev):
@@ -708,10 +901,13 @@ def run_omnigs(args, rank, world, local_rank):
 
     batched = None
     extra = None
-    if world == 1 and not args.no_batch and (P, W, H) == (P_GAUSS, WIDTH, HEIGHT):
+    headline = (P, W, H) == (P_GAUSS, WIDTH, HEIGHT)
+    if world == 1 and not args.no_batch and headline:
         batched = run_batched(args, g, gt, dev, value)
-        if not args.no_extra:
-            extra = {"precision": run_precision(args, dev), "peak_memory": run_peak_memory(dev)}
+    if world == 1 and not args.no_extra and headline:
+        extra = {"precision": run_precision(args, dev), "peak_memory": run_peak_memory(dev),
+                 "differentiation": run_differentiation(args, dev)}
+
 
     cpu = None
     if rank == 0 and world == 1 and not args.no_cpu_baseline:

@@ -54,14 +54,20 @@ def _run(cmd, verbose):
 
 
 def build_capi(verbose: bool = False, force: bool = False) -> str:
+    from concurrent.futures import ThreadPoolExecutor
+
     os.makedirs(OBJ_DIR, exist_ok=True)
-    objs = []
+    objs, jobs = [], []
     for src in CU_SOURCES:
         path = os.path.join(CSRC, src)
         obj = os.path.join(OBJ_DIR, src.replace(".cu", ".o"))
         objs.append(obj)
         if force or _newer(obj, [path] + HEADERS):
-            _run([NVCC, *ARCH, *NVCC_FLAGS, "-c", path, "-o", obj], verbose)
+            jobs.append([NVCC, *ARCH, *NVCC_FLAGS, "-c", path, "-o", obj])
+    # one nvcc per source, as many at once as there are cores
+    with ThreadPoolExecutor(max_workers=max(1, os.cpu_count() or 1)) as pool:
+        for f in [pool.submit(_run, cmd, verbose) for cmd in jobs]:
+            f.result()
     if force or _newer(CAPI_LIB, objs):
         _run([NVCC, *ARCH, "-shared", "-o", CAPI_LIB, *objs, "-lcudart"], verbose)
     return CAPI_LIB
