@@ -25,8 +25,9 @@ across ranks every step with one NCCL all-reduce, as a data-parallel train step 
 * cpu_baseline: the FP64 oracle (multithreaded C++ restatement of the reference algorithm) on the
   same view, on this host's cores.
 * configs: the precision configuration (6M pole-heavy Gaussians, 4096x2048), peak memory at
-  4096x2048 over 3M Gaussians, and the differentiation configuration (500 Adam steps over 24 views
-  through the LibTorch autograd Function).
+  4096x2048 over 3M Gaussians (stored and recomputed transmittance), the headline view with
+  transmittance checkpointing, and the differentiation configuration (500 Adam steps over 24
+  views through the LibTorch autograd Function).
 * --impl reference: the reference arm.  The reference's rasterizer is CUDA-only, so its CPU
   implementation of the path is the FP64 oracle port, timed here on all host cores.  The same line
   carries reference_gpu: the reference's own CUDA rasterizer rebuilt for sm_100a
@@ -471,9 +472,9 @@ def run_precision(args, dev):
 
 
 def run_peak_memory(dev):
-    """Peak device memory of one fwd+bwd at 4096x2048 over 3M Gaussians through the plain path
-    (transmittance is recomputed in the backward: per pixel only final T and the last-contributor
-    index are stored)."""
+    """Peak device memory of one fwd+bwd at 4096x2048 over 3M Gaussians through the plain path,
+    with the per-pixel state stored (final T and last contributor, 8 B per pixel) and with
+    transmittance checkpointing (recomputed in the backward, nothing stored per pixel)."""
     import torch
 
     from omnigs_b200 import lonlat, scenes
@@ -483,20 +484,50 @@ def run_peak_memory(dev):
     gt = lonlat.GaussianTensors.from_numpy(g, dev)
     cam = lonlat.Camera.from_view(scenes.identity_view(W, H), dev)
     dpix = torch.from_numpy(scenes.upstream_grad(W, H, seed=3)).to(dev)
-    torch.cuda.synchronize()
-    base = torch.cuda.memory_allocated(dev)
-    torch.cuda.reset_peak_memory_stats(dev)
-    img, radii, n, state = lonlat.rasterize(gt, cam, capacity=1)  # exact sizing (one resize)
-    grads = lonlat.Gradients.empty(P, 16, dev)
-    state.backward(gt, cam, radii, dpix, grads, R=n)
-    torch.cuda.synchronize()
-    peak = torch.cuda.max_memory_allocated(dev) - base
-    per_pixel_state = 8 * W * H
-    out = {"workload": "3M Gaussians, one 4096x2048 view, fwd+bwd (plain path)", "num_rendered": int(n),
-           "peak_bytes_above_inputs": int(peak), "peak_gb": round(peak / 1e9, 3),
-           "per_pixel_state_bytes": per_pixel_state}
-    del state, grads, img, gt
+    out = {"workload": "3M Gaussians, one 4096x2048 view, fwd+bwd (plain path)"}
+    for key, recompute in (("stored_T", False), ("recompute_T", True)):
+        torch.cuda.synchronize()
+        torch.cuda.empty_cache()
+        base = torch.cuda.memory_allocated(dev)
+        torch.cuda.reset_peak_memory_stats(dev)
+        img, radii, n, state = lonlat.rasterize(gt, cam, capacity=1, recompute_T=recompute)  # exact sizing
+        grads = lonlat.Gradients.empty(P, 16, dev)
+        state.backward(gt, cam, radii, dpix, grads, R=n)
+        torch.cuda.synchronize()
+        peak = torch.cuda.max_memory_allocated(dev) - base
+        out["num_rendered"] = int(n)
+        out[key] = {"peak_bytes_above_inputs": int(peak), "peak_gb": round(peak / 1e9, 3),
+                    "image_state_bytes": int(state.image.numel())}
+        del state, grads, img, radii
+    out["per_pixel_state_bytes"] = 8 * W * H
+    del gt
     torch.cuda.empty_cache()
+    return out
+
+
+def run_checkpointing(args, gt, cam, dpix, n0, dev):
+    """Headline view (1M Gaussians, 2048x1024) fwd+bwd with transmittance checkpointing: the forward
+    stores no per-pixel state and the backward replays the forward's recurrence per tile."""
+    import torch
+
+    from omnigs_b200 import lonlat
+
+    P, W, H = gt.P, cam.width, cam.height
+    out = {}
+    for key, recompute in (("stored_T_ms_per_view", False), ("recompute_T_ms_per_view", True)):
+        state = lonlat.LonlatState(P, W, H, n0 + n0 // 8 + 4096, dev, recompute_T=recompute)
+        img = torch.empty(3, H, W, device=dev)
+        radii = torch.empty(P, dtype=torch.int32, device=dev)
+        grads = lonlat.Gradients.empty(P, 16, dev)
+
+        def step():
+            state.forward(gt, cam, img, radii)
+            state.backward(gt, cam, radii, dpix, grads)
+
+        out[key] = _time_steps(step, args, dev)
+        del state, grads, img, radii
+    torch.cuda.empty_cache()
+    out["saved_bytes_per_pixel"] = 8
     return out
 
 
@@ -906,6 +937,7 @@ def run_omnigs(args, rank, world, local_rank):
         batched = run_batched(args, g, gt, dev, value)
     if world == 1 and not args.no_extra and headline:
         extra = {"precision": run_precision(args, dev), "peak_memory": run_peak_memory(dev),
+                 "checkpointing": run_checkpointing(args, gt, cam, dpix, n0, dev),
                  "differentiation": run_differentiation(args, dev)}
 
 

@@ -52,6 +52,16 @@ typedef struct CUstream_st* omnigs_stream_t; /* same type as cudaStream_t */
 #define OMNIGS_CAMERA_PINHOLE 1
 #define OMNIGS_CAMERA_LONLAT 3
 
+/* Bits of the forward/backward `flags` field.
+ * OMNIGS_FLAG_RECOMPUTE_T: transmittance checkpointing.  The forward keeps no per-pixel state (the
+ * image buffer, omnigs_lonlat_image_bytes_flags(W, H, OMNIGS_FLAG_RECOMPUTE_T), holds only the tile
+ * ranges) and the backward recomputes each pixel's final transmittance and last contributor by
+ * replaying the forward's front-to-back recurrence over the tile (bit-identical to the stored
+ * values), saving 8 bytes per pixel for the cost of that replay.  The forward and the backward of
+ * one rasterization must use the same flags.  No counterpart in the reference, which stores them
+ * (ImageState, rasterizer_impl.h:48-90). */
+#define OMNIGS_FLAG_RECOMPUTE_T 1
+
 /* Inputs and outputs of one forward rasterization.
  * Replaces the argument list of CudaRasterizer::LonlatRasterizer::forward
  * (cuda_rasterizer/rasterizer.h:104-123) as called from src/rasterize_points.cu:136-155. */
@@ -73,6 +83,7 @@ typedef struct OmnigsLonlatForwardArgs {
   const float* campos;        /* [3] */
   float* out_color;           /* [3,H,W] output */
   int* radii;                 /* [P] output */
+  int flags;                  /* OMNIGS_FLAG_* (0: the reference's stored per-pixel state) */
 } OmnigsLonlatForwardArgs;
 
 /* Inputs and outputs of one backward pass.
@@ -103,6 +114,7 @@ typedef struct OmnigsLonlatBackwardArgs {
   float* dL_dscales;          /* [P,3] */
   float* dL_drotations;       /* [P,4] */
   float* dL_dconic;           /* [P,4] (x, y, 0, w) or NULL; internal in the reference */
+  int flags;                  /* OMNIGS_FLAG_*, as given to the forward */
 } OmnigsLonlatBackwardArgs;
 
 /* Library version string. */
@@ -116,6 +128,8 @@ const char* omnigs_last_error(void);
  * largest num_rendered it can hold. */
 size_t omnigs_lonlat_geom_bytes(int P);
 size_t omnigs_lonlat_image_bytes(int W, int H);
+/* Image buffer size for the given OMNIGS_FLAG_* bits (with OMNIGS_FLAG_RECOMPUTE_T: tile ranges only). */
+size_t omnigs_lonlat_image_bytes_flags(int W, int H, int flags);
 size_t omnigs_lonlat_binning_bytes(int64_t capacity);
 int64_t omnigs_lonlat_binning_capacity(size_t binning_bytes);
 

@@ -22,6 +22,12 @@ _HERE = os.path.dirname(os.path.abspath(__file__))
 _ext = None
 
 
+def set_recompute_transmittance(on: bool) -> None:
+    """Transmittance checkpointing for the following LibTorch-layer forwards of this process: no
+    per-pixel state is stored and the backward recomputes it (OMNIGS_FLAG_RECOMPUTE_T)."""
+    torch_ext().set_recompute_transmittance(bool(on))
+
+
 def torch_ext():
     """Import the LibTorch extension (omnigs_b200/lib/_omnigs_torch*.so); raises if not built."""
     global _ext

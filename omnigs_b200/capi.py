@@ -33,7 +33,7 @@ class ForwardArgs(ctypes.Structure):
                 ("background", _vp), ("means3D", _vp), ("shs", _vp), ("colors_precomp", _vp),
                 ("opacities", _vp), ("scales", _vp), ("scale_modifier", _f), ("rotations", _vp),
                 ("cov3D_precomp", _vp), ("viewmatrix", _vp), ("campos", _vp),
-                ("out_color", _vp), ("radii", _vp)]
+                ("out_color", _vp), ("radii", _vp), ("flags", _i)]
 
 
 class BackwardArgs(ctypes.Structure):
@@ -43,7 +43,7 @@ class BackwardArgs(ctypes.Structure):
                 ("viewmatrix", _vp), ("campos", _vp), ("radii", _vp), ("dL_dout_color", _vp),
                 ("dL_dmeans2D", _vp), ("dL_dcolors", _vp), ("dL_dopacity", _vp),
                 ("dL_dmeans3D", _vp), ("dL_dcov3D", _vp), ("dL_dsh", _vp), ("dL_dscales", _vp),
-                ("dL_drotations", _vp), ("dL_dconic", _vp)]
+                ("dL_drotations", _vp), ("dL_dconic", _vp), ("flags", _i)]
 
 
 STAGES = ["preprocess", "duplicate", "sort", "ranges", "render_forward", "render_backward",
@@ -124,7 +124,7 @@ class TuneResult(ctypes.Structure):
 
 # every symbol include/omnigs_b200.h declares
 EXPORTED = ["omnigs_version", "omnigs_last_error", "omnigs_lonlat_geom_bytes",
-            "omnigs_lonlat_image_bytes", "omnigs_lonlat_binning_bytes",
+            "omnigs_lonlat_image_bytes", "omnigs_lonlat_image_bytes_flags", "omnigs_lonlat_binning_bytes",
             "omnigs_lonlat_binning_capacity", "omnigs_lonlat_preprocess", "omnigs_lonlat_render",
             "omnigs_lonlat_forward", "omnigs_lonlat_forward_noalloc", "omnigs_lonlat_forward_early_status",
             "omnigs_lonlat_read_status",
@@ -153,6 +153,8 @@ def lib() -> ctypes.CDLL:
         L.omnigs_lonlat_geom_bytes.argtypes = [_i]
         L.omnigs_lonlat_image_bytes.restype = ctypes.c_size_t
         L.omnigs_lonlat_image_bytes.argtypes = [_i, _i]
+        L.omnigs_lonlat_image_bytes_flags.restype = ctypes.c_size_t
+        L.omnigs_lonlat_image_bytes_flags.argtypes = [_i, _i, _i]
         L.omnigs_lonlat_binning_bytes.restype = ctypes.c_size_t
         L.omnigs_lonlat_binning_bytes.argtypes = [ctypes.c_int64]
         L.omnigs_lonlat_binning_capacity.restype = ctypes.c_int64
@@ -232,8 +234,11 @@ def geom_bytes(P: int) -> int:
     return int(lib().omnigs_lonlat_geom_bytes(P))
 
 
-def image_bytes(W: int, H: int) -> int:
-    return int(lib().omnigs_lonlat_image_bytes(W, H))
+FLAG_RECOMPUTE_T = 1  # OMNIGS_FLAG_RECOMPUTE_T
+
+
+def image_bytes(W: int, H: int, flags: int = 0) -> int:
+    return int(lib().omnigs_lonlat_image_bytes_flags(W, H, flags))
 
 
 def binning_bytes(capacity: int) -> int:

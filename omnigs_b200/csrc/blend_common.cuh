@@ -143,7 +143,8 @@ __device__ __forceinline__ float2 splat_power2(const float4& a, const float4& b,
 }
 
 // Stages instances [base, base + cnt) of the tile's list (from the back when reverse: slot t holds
-// position base_hi - 1 - t, with base the exclusive upper end) into shared memory.
+// position base_hi - 1 - t, with base the exclusive upper end) into shared memory; s_c (colour) and
+// s_g (record index) may be NULL.
 __device__ __forceinline__ void stage_batch(const BlendSource& src, uint32_t range_begin, int base, int cnt,
                                             bool reverse, float4* s_a, float4* s_b, float4* s_c,
                                             uint32_t* s_g) {
@@ -154,12 +155,90 @@ __device__ __forceinline__ void stage_batch(const BlendSource& src, uint32_t ran
       if (s_g) s_g[t] = g;
       s_a[t] = src.splat[2 * g];
       s_b[t] = src.splat[2 * g + 1];
-      s_c[t] = src.color[g];
-    } else {  // unreachable for a consistent instance list; stage a splat that never contributes
+      if (s_c) s_c[t] = src.color[g];
+    } else {  // unreachable for a consistent instance list; stage a splat that never contributes:
+              // finite, unit conic, threshold -inf (no patch test hits), opacity 0 (alpha 0)
       if (s_g) s_g[t] = 0;
-      s_a[t] = make_float4(__int_as_float(0x7f800000), 0.f, 0.f, 0.f);
-      s_b[t] = make_float4(0.f, 0.f, -__int_as_float(0x7f800000), -__int_as_float(0x7f800000));
-      s_c[t] = make_float4(0.f, 0.f, 0.f, 0.f);
+      s_a[t] = make_float4(0.f, 0.f, 1.f, 0.f);
+      s_b[t] = make_float4(1.f, 0.f, -__int_as_float(0x7f800000), 1.f);
+      if (s_c) s_c[t] = make_float4(0.f, 0.f, 0.f, 0.f);
+    }
+  }
+}
+
+// The forward's front-to-back pass over a tile's instances (forward.cu:394-456) for the thread's two
+// pixels (lane x: row py0, lane y: row py0 + 4): transmittance T and last contributor lc, and with
+// kColor the blended colour C.  Every pixel evaluates the reference's per-pair arithmetic and control
+// flow (power, alpha = min(0.99, o exp(power)), the 1/255 skip, the T < 1e-4 stop), so T and lc are
+// the same whether or not colour is blended: the forward kernel runs it with colour, the backward
+// runs it without to recompute the state it did not store.  The staging arrays hold kBatch splats.
+// The block's threads must all call it (it synchronises the block).
+template <int kBatch, bool kWrap, bool kColor>
+__device__ __forceinline__ void forward_pass(const TileJob& job, const BlendSource& src, const BlendPatch& patch,
+                                             float4* s_a, float4* s_b, float4* s_c, float2& T, uint32_t& lc0,
+                                             uint32_t& lc1, float2& C0, float2& C1, float2& C2) {
+  static_assert(kBlendPx == 2, "the blend packs a thread's two pixels into f32x2 lanes");
+  const int lane = threadIdx.x & 31;
+  const uint2 range = job.range;
+  const int n = (int)(range.y - range.x);
+  bool done0 = !patch.inside(0, job.W, job.H), done1 = !patch.inside(1, job.W, job.H);
+  T = f2(1.0f);
+  C0 = C1 = C2 = f2(0.f);
+  lc0 = lc1 = 0;
+  const float2 pyf = make_float2(patch.pyf(0), patch.pyf(1));
+
+  for (int base = 0; base < n; base += kBatch) {
+    if (__syncthreads_and(done0 && done1)) break;
+    stage_batch(src, range.x, base, min(kBatch, n - base), /*reverse=*/false, s_a, s_b, kColor ? s_c : nullptr,
+                nullptr);
+    __syncthreads();
+    const int cnt = min(kBatch, n - base);
+    bool warp_done = __all_sync(kFullMask, done0 && done1);
+    for (int k = 0; k * 32 < cnt && !warp_done; ++k) {
+      const int j = k * 32 + lane;
+      bool hit = false;
+      if (j < cnt) hit = patch.template hit<kWrap>(s_a[j], s_b[j]);
+      unsigned m = __ballot_sync(kFullMask, hit);
+      while (m) {
+        const int jj = k * 32 + __ffs(m) - 1;
+        m &= m - 1;
+        if (!(done0 && done1)) {
+          const float4 a = s_a[jj];
+          const float4 b = s_b[jj];
+          const float dx = patch.template center_x<kWrap>(a.x) - patch.pxf;
+          const float2 dy = sub2(f2(a.y), pyf);
+          const float2 power = splat_power2(a, b, dx, dy);
+          const float2 alpha = make_float2(fminf(0.99f, b.y * expf(power.x)), fminf(0.99f, b.y * expf(power.y)));
+          bool act0 = !done0 && !(power.x > 0.0f) && !(alpha.x < 1.0f / 255.0f);
+          bool act1 = !done1 && !(power.y > 0.0f) && !(alpha.y < 1.0f / 255.0f);
+          if (act0 || act1) {
+            const float2 test_T = mul2(T, sub2(f2(1.0f), alpha));
+            // a pixel whose transmittance would fall below 1e-4 stops without this splat
+            if (act0 && test_T.x < 0.0001f) {
+              done0 = true;
+              act0 = false;
+            }
+            if (act1 && test_T.y < 0.0001f) {
+              done1 = true;
+              act1 = false;
+            }
+            if (kColor) {
+              const float2 ae = make_float2(act0 ? alpha.x : 0.f, act1 ? alpha.y : 0.f);
+              const float4 c = s_c[jj];
+              // C += colour * alpha * T, rounded as the reference's compiled blend (fused add);
+              // a pixel without this splat adds exactly 0
+              C0 = fma2(mul2(f2(c.x), ae), T, C0);
+              C1 = fma2(mul2(f2(c.y), ae), T, C1);
+              C2 = fma2(mul2(f2(c.z), ae), T, C2);
+            }
+            T = make_float2(act0 ? test_T.x : T.x, act1 ? test_T.y : T.y);
+            const uint32_t idx = (uint32_t)(base + jj + 1);
+            lc0 = act0 ? idx : lc0;
+            lc1 = act1 ? idx : lc1;
+          }
+        }
+      }
+      warp_done = __all_sync(kFullMask, done0 && done1);
     }
   }
 }

@@ -94,8 +94,12 @@ int validate_forward(const OmnigsLonlatForwardArgs* a) {
     return fail(OMNIGS_ERR_INVALID_ARGUMENT, "out_color and background are required");
   if (a->P > 0 && (a->radii == nullptr || a->opacities == nullptr))
     return fail(OMNIGS_ERR_INVALID_ARGUMENT, "radii and opacities are required");
+  if (a->flags & ~OMNIGS_FLAG_RECOMPUTE_T) return fail(OMNIGS_ERR_INVALID_ARGUMENT, "unknown flags");
   return OMNIGS_OK;
 }
+
+// Per-pixel state is stored unless the caller asked for transmittance checkpointing.
+bool stores_state(int flags) { return (flags & OMNIGS_FLAG_RECOMPUTE_T) == 0; }
 
 __global__ void mark_visible_kernel(int P, const float* means3D, const float* vm, int camera_type,
                                     uint8_t* present) {
@@ -139,6 +143,11 @@ size_t omnigs_lonlat_geom_bytes(int P) { return GeomLayout::make(P < 0 ? 0 : P).
 size_t omnigs_lonlat_image_bytes(int W, int H) {
   if (W <= 0 || H <= 0) return 0;
   return ImageLayout::make(W, H).total;
+}
+
+size_t omnigs_lonlat_image_bytes_flags(int W, int H, int flags) {
+  if (W <= 0 || H <= 0) return 0;
+  return ImageLayout::make(W, H, stores_state(flags)).total;
 }
 
 size_t omnigs_lonlat_binning_bytes(int64_t capacity) {
@@ -241,11 +250,11 @@ int render_impl(const OmnigsLonlatForwardArgs* a, void* geom, size_t geom_bytes,
     return OMNIGS_OK;
   }
   const GeomLayout GL = GeomLayout::make(a->P);
-  const ImageLayout IL = ImageLayout::make(a->W, a->H);
+  const ImageLayout IL = ImageLayout::make(a->W, a->H, stores_state(a->flags));
   if (geom == nullptr || geom_bytes < GL.total)
     return fail(OMNIGS_ERR_BUFFER_TOO_SMALL, "geometry buffer smaller than omnigs_lonlat_geom_bytes(P)");
   if (image == nullptr || image_bytes < IL.total)
-    return fail(OMNIGS_ERR_BUFFER_TOO_SMALL, "image buffer smaller than omnigs_lonlat_image_bytes(W, H)");
+    return fail(OMNIGS_ERR_BUFFER_TOO_SMALL, "image buffer smaller than omnigs_lonlat_image_bytes_flags(W, H, flags)");
   int64_t capacity = BinningLayout::capacity_for(binning_bytes);
   if (binning == nullptr || capacity < 0)
     return fail(OMNIGS_ERR_BUFFER_TOO_SMALL, "binning buffer smaller than omnigs_lonlat_binning_bytes(0)");
@@ -372,8 +381,8 @@ int render_impl(const OmnigsLonlatForwardArgs* a, void* geom, size_t geom_bytes,
   r.color = at<float4>(geom, GL.color);
   r.bg = a->background;
   r.out_color = a->out_color;
-  r.final_T = at<float>(image, IL.final_T);
-  r.n_contrib = at<uint32_t>(image, IL.n_contrib);
+  r.final_T = IL.store_state ? at<float>(image, IL.final_T) : nullptr;
+  r.n_contrib = IL.store_state ? at<uint32_t>(image, IL.n_contrib) : nullptr;
   if (early != nullptr) {
     if (cudaMemcpyAsync(early->host, hdr, sizeof(GeomHeader), cudaMemcpyDeviceToHost, s) != cudaSuccess ||
         cudaEventRecord(early->copied, s) != cudaSuccess)
@@ -465,6 +474,7 @@ int omnigs_lonlat_backward(const OmnigsLonlatBackwardArgs* a, void* geom, size_t
   if (int rc = validate_common(a->P, a->D, a->M, a->W, a->H, a->shs, a->colors_precomp, a->scales,
                                a->rotations, a->cov3D_precomp, a->means3D, a->viewmatrix, a->campos))
     return rc;
+  if (a->flags & ~OMNIGS_FLAG_RECOMPUTE_T) return fail(OMNIGS_ERR_INVALID_ARGUMENT, "unknown flags");
   if (a->P == 0) return OMNIGS_OK;
   if (a->radii == nullptr || a->dL_dout_color == nullptr || a->background == nullptr ||
       a->dL_dmeans2D == nullptr || a->dL_dcolors == nullptr || a->dL_dopacity == nullptr ||
@@ -473,11 +483,11 @@ int omnigs_lonlat_backward(const OmnigsLonlatBackwardArgs* a, void* geom, size_t
     return fail(OMNIGS_ERR_INVALID_ARGUMENT, "a required backward input or output is NULL");
   cudaStream_t s = reinterpret_cast<cudaStream_t>(stream);
   const GeomLayout GL = GeomLayout::make(a->P);
-  const ImageLayout IL = ImageLayout::make(a->W, a->H);
+  const ImageLayout IL = ImageLayout::make(a->W, a->H, stores_state(a->flags));
   if (geom == nullptr || geom_bytes < GL.total)
     return fail(OMNIGS_ERR_BUFFER_TOO_SMALL, "geometry buffer smaller than omnigs_lonlat_geom_bytes(P)");
   if (image == nullptr || image_bytes < IL.total)
-    return fail(OMNIGS_ERR_BUFFER_TOO_SMALL, "image buffer smaller than omnigs_lonlat_image_bytes(W, H)");
+    return fail(OMNIGS_ERR_BUFFER_TOO_SMALL, "image buffer smaller than omnigs_lonlat_image_bytes_flags(W, H, flags)");
   const int64_t capacity = BinningLayout::capacity_for(binning_bytes);
   if (binning == nullptr || capacity < 0)
     return fail(OMNIGS_ERR_BUFFER_TOO_SMALL, "binning buffer smaller than omnigs_lonlat_binning_bytes(0)");
@@ -498,8 +508,9 @@ int omnigs_lonlat_backward(const OmnigsLonlatBackwardArgs* a, void* geom, size_t
   r.splat = at<float4>(geom, GL.splat);
   r.color = at<float4>(geom, GL.color);
   r.bg = a->background;
-  r.final_T = const_cast<float*>(at<float>(image, IL.final_T));
-  r.n_contrib = const_cast<uint32_t*>(at<uint32_t>(image, IL.n_contrib));
+  // NULL per-pixel state: the backward blend recomputes it (transmittance checkpointing)
+  r.final_T = IL.store_state ? const_cast<float*>(at<float>(image, IL.final_T)) : nullptr;
+  r.n_contrib = IL.store_state ? const_cast<uint32_t*>(at<uint32_t>(image, IL.n_contrib)) : nullptr;
   r.dL_dpix = a->dL_dout_color;
   r.grad_acc = at<float>(geom, GL.grad_acc);
   staged(OMNIGS_STAGE_RENDER_BACKWARD, 1, s, [&] { launch_render_backward(r, s); });

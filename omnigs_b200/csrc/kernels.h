@@ -125,8 +125,8 @@ struct RenderParams {
   const float4* color;
   const float* bg;
   float* out_color;
-  float* final_T;
-  uint32_t* n_contrib;
+  float* final_T;       // NULL with transmittance checkpointing: the forward does not store it and
+  uint32_t* n_contrib;  // the backward recomputes it
   // backward only
   const float* dL_dpix;
   float* grad_acc;  // [P][12]

@@ -12,7 +12,8 @@
 //                                tiles_touched u32[P] | depth-sort keys/values u32[4][P] |
 //                                gradient accumulators float4[3P]
 //   image (per pixel, N = W*H):  final transmittance f32[N] | last contributor u32[N] |
-//                                tile ranges uint2[tiles]
+//                                tile ranges uint2[tiles]  (tile ranges only with
+//                                OMNIGS_FLAG_RECOMPUTE_T: the backward recomputes the rest)
 //   binning (per instance, capacity C): tile keys u32[2][C] | Gaussian indices u32[2][C] |
 //                                digit histograms u32[7][256] | tile-sort look-back u32[3][tiles][256]
 //
@@ -90,13 +91,16 @@ struct GeomLayout {
   }
 };
 
+// With store_state false (transmittance checkpointing) the buffer holds only the tile ranges.
 struct ImageLayout {
   size_t final_T, n_contrib, ranges, total;
-  static ImageLayout make(int W, int H) {
+  bool store_state;
+  static ImageLayout make(int W, int H, bool store_state = true) {
     ImageLayout L;
-    const int64_t N = (int64_t)W * H;
+    const int64_t N = store_state ? (int64_t)W * H : 0;
     const int64_t tiles = (int64_t)tiles_x(W) * tiles_y(H);
     size_t o = 0;
+    L.store_state = store_state;
     L.final_T = o; o = align_up(o + sizeof(float) * N);
     L.n_contrib = o; o = align_up(o + sizeof(uint32_t) * N);
     L.ranges = o; o = align_up(o + sizeof(uint32_t) * 2 * tiles);

@@ -8,9 +8,9 @@
 // per block), so nothing is copied to the host (the reference copies num_rendered back between
 // its scan and its duplication, rasterizer_impl.cu:622-628).
 //
-// Besides the reference's outputs, each visible splat gets the half-extents of the axis-aligned
-// box outside which its alpha is provably below 1/255; the blend kernels use them to skip a splat
-// for a whole warp without changing any per-pixel decision.
+// Besides the reference's outputs, each visible splat gets the threshold of its quadratic form
+// beyond which its alpha is provably below 1/255 and its conic's determinant; the blend kernels use
+// them to skip a splat for a whole warp without changing any per-pixel decision.
 #include "kernels.h"
 #include "preprocess_common.cuh"
 #include "sh_io.cuh"

@@ -57,7 +57,10 @@ __device__ __forceinline__ float rcp_approx(float x) {
 // Eight resident blocks per SM (at most 64 registers per thread) measured fastest on a B200.
 constexpr int kBlendBwdMinBlocks = 8;
 
-template <int kBatch, bool kWrap>
+// kRecompute (transmittance checkpointing): the forward stored no per-pixel state; each pixel's
+// final transmittance and last contributor are recomputed first by the forward's own front-to-back
+// pass without colour (forward_pass), which yields the values the forward would have stored.
+template <int kBatch, bool kWrap, bool kRecompute>
 __device__ __forceinline__ void blend_backward_tile(const TileJob& job, const BlendSource& src, float* grad_acc) {
   static_assert(kBlendPx == 2, "the backward blend packs a thread's two pixels into f32x2 lanes");
   __shared__ float4 s_a[kBatch];
@@ -79,12 +82,23 @@ __device__ __forceinline__ void blend_backward_tile(const TileJob& job, const Bl
   const int64_t HW = (int64_t)job.H * job.W;
   float Tf[2], dp[3][2];
   uint32_t lc[2];
+  if (kRecompute) {
+    float2 Tr, c0, c1, c2;
+    uint32_t l0, l1;
+    forward_pass<kBatch, kWrap, false>(job, src, patch, s_a, s_b, nullptr, Tr, l0, l1, c0, c1, c2);
+    Tf[0] = patch.inside(0, job.W, job.H) ? Tr.x : 0.f;
+    Tf[1] = patch.inside(1, job.W, job.H) ? Tr.y : 0.f;
+    lc[0] = min(l0, n);
+    lc[1] = min(l1, n);
+  }
 #pragma unroll
   for (int i = 0; i < 2; ++i) {
     const bool in = patch.inside(i, job.W, job.H);
     const int64_t pix = in ? patch.pixel(i, job.W) : 0;
-    Tf[i] = in ? job.final_T[pix] : 0.f;
-    lc[i] = in ? min(job.n_contrib[pix], n) : 0u;
+    if (!kRecompute) {
+      Tf[i] = in ? job.final_T[pix] : 0.f;
+      lc[i] = in ? min(job.n_contrib[pix], n) : 0u;
+    }
 #pragma unroll
     for (int ch = 0; ch < 3; ++ch) dp[ch][i] = in ? job.dL_dpix[ch * HW + pix] : 0.f;
   }
@@ -197,7 +211,7 @@ __device__ __forceinline__ void blend_backward_tile(const TileJob& job, const Bl
 }
 
 // One view: block (x, y) back-propagates tile (x, y).
-template <int kBatch>
+template <int kBatch, bool kRecompute>
 __global__ void __launch_bounds__(kBlendThreads, kBlendBwdMinBlocks) render_backward_kernel(RenderParams p) {
   TileJob job;
   job.tile_x = blockIdx.x;
@@ -211,15 +225,16 @@ __global__ void __launch_bounds__(kBlendThreads, kBlendBwdMinBlocks) render_back
   job.n_contrib = p.n_contrib;
   job.dL_dpix = p.dL_dpix;
   job.wrap_w = 0.f;
-  blend_backward_tile<kBatch, false>(job, BlendSource{p.point_list, p.splat, p.color, (uint32_t)p.P, p.capacity}, p.grad_acc);
+  blend_backward_tile<kBatch, false, kRecompute>(job, BlendSource{p.point_list, p.splat, p.color, (uint32_t)p.P, p.capacity},
+                                                 p.grad_acc);
 }
 
 // All views of a batch in one launch: block b back-propagates global tile b.
 template <int kBatch, bool kWrap>
 __global__ void __launch_bounds__(kBlendThreads, kBlendBwdMinBlocks) batch_render_backward_kernel(const __grid_constant__ BatchRenderParams p) {
   const TileJob job = batch_tile_job(p, blockIdx.x);
-  blend_backward_tile<kBatch, kWrap>(job, BlendSource{p.point_list, p.splat, p.color, (uint32_t)p.P * (uint32_t)p.V, p.capacity},
-                      p.grad_acc);
+  blend_backward_tile<kBatch, kWrap, false>(job, BlendSource{p.point_list, p.splat, p.color, (uint32_t)p.P * (uint32_t)p.V, p.capacity},
+                                            p.grad_acc);
 }
 
 template <bool kWrap>
@@ -231,16 +246,24 @@ void launch_batch_blend(const BatchRenderParams& p, cudaStream_t s) {
   }
 }
 
+template <bool kRecompute>
+void launch_single_view_backward(const RenderParams& p, const dim3 grid, cudaStream_t s) {
+  switch (blend_batch_size(true)) {
+    case 128: render_backward_kernel<128, kRecompute><<<grid, kBlendThreads, 0, s>>>(p); break;
+    case 512: render_backward_kernel<512, kRecompute><<<grid, kBlendThreads, 0, s>>>(p); break;
+    default: render_backward_kernel<256, kRecompute><<<grid, kBlendThreads, 0, s>>>(p); break;
+  }
+}
+
 }  // namespace
 
 void launch_render_backward(const RenderParams& p, cudaStream_t s) {
   if (p.gx <= 0 || p.gy <= 0) return;
   const dim3 grid(p.gx, p.gy);
-  switch (blend_batch_size(true)) {
-    case 128: render_backward_kernel<128><<<grid, kBlendThreads, 0, s>>>(p); break;
-    case 512: render_backward_kernel<512><<<grid, kBlendThreads, 0, s>>>(p); break;
-    default: render_backward_kernel<256><<<grid, kBlendThreads, 0, s>>>(p); break;
-  }
+  if (p.final_T == nullptr)  // transmittance checkpointing: recompute the per-pixel state
+    launch_single_view_backward<true>(p, grid, s);
+  else
+    launch_single_view_backward<false>(p, grid, s);
 }
 
 void launch_batch_render_backward(const BatchRenderParams& p, cudaStream_t s) {

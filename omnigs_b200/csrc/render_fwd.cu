@@ -24,72 +24,13 @@ namespace {
 
 template <int kBatch, bool kWrap>
 __device__ __forceinline__ void blend_forward_tile(const TileJob& job, const BlendSource& src) {
-  static_assert(kBlendPx == 2, "the forward blend packs a thread's two pixels into f32x2 lanes");
   __shared__ float4 s_a[kBatch];  // x, y, conic a, conic b
-  __shared__ float4 s_b[kBatch];  // conic c, opacity, cull half-width, cull half-height
+  __shared__ float4 s_b[kBatch];  // conic c, opacity, cull threshold, conic determinant
   __shared__ float4 s_c[kBatch];  // r, g, b, clamp bits
   const BlendPatch patch = BlendPatch::make(job.tile_x, job.tile_y, job.wrap_w);
-  const int lane = threadIdx.x & 31;
-  const uint2 range = job.range;
-  const int n = (int)(range.y - range.x);
-
-  // lane x: row py0, lane y: row py0 + 4
-  bool done0 = !patch.inside(0, job.W, job.H), done1 = !patch.inside(1, job.W, job.H);
-  float2 T = f2(1.0f), C0 = f2(0.f), C1 = f2(0.f), C2 = f2(0.f);
-  uint32_t lc0 = 0, lc1 = 0;
-  const float2 pyf = make_float2(patch.pyf(0), patch.pyf(1));
-
-  for (int base = 0; base < n; base += kBatch) {
-    if (__syncthreads_and(done0 && done1)) break;
-    stage_batch(src, range.x, base, min(kBatch, n - base), /*reverse=*/false, s_a, s_b, s_c, nullptr);
-    __syncthreads();
-    const int cnt = min(kBatch, n - base);
-    bool warp_done = __all_sync(kFullMask, done0 && done1);
-    for (int k = 0; k * 32 < cnt && !warp_done; ++k) {
-      const int j = k * 32 + lane;
-      bool hit = false;
-      if (j < cnt) hit = patch.template hit<kWrap>(s_a[j], s_b[j]);
-      unsigned m = __ballot_sync(kFullMask, hit);
-      while (m) {
-        const int jj = k * 32 + __ffs(m) - 1;
-        m &= m - 1;
-        if (!(done0 && done1)) {
-          const float4 a = s_a[jj];
-          const float4 b = s_b[jj];
-          const float dx = patch.template center_x<kWrap>(a.x) - patch.pxf;
-          const float2 dy = sub2(f2(a.y), pyf);
-          const float2 power = splat_power2(a, b, dx, dy);
-          const float2 alpha = make_float2(fminf(0.99f, b.y * expf(power.x)), fminf(0.99f, b.y * expf(power.y)));
-          bool act0 = !done0 && !(power.x > 0.0f) && !(alpha.x < 1.0f / 255.0f);
-          bool act1 = !done1 && !(power.y > 0.0f) && !(alpha.y < 1.0f / 255.0f);
-          if (act0 || act1) {
-            const float2 test_T = mul2(T, sub2(f2(1.0f), alpha));
-            // a pixel whose transmittance would fall below 1e-4 stops without this splat
-            if (act0 && test_T.x < 0.0001f) {
-              done0 = true;
-              act0 = false;
-            }
-            if (act1 && test_T.y < 0.0001f) {
-              done1 = true;
-              act1 = false;
-            }
-            const float2 ae = make_float2(act0 ? alpha.x : 0.f, act1 ? alpha.y : 0.f);
-            const float4 c = s_c[jj];
-            // C += colour * alpha * T, rounded as the reference's compiled blend (fused add);
-            // a pixel without this splat adds exactly 0
-            C0 = fma2(mul2(f2(c.x), ae), T, C0);
-            C1 = fma2(mul2(f2(c.y), ae), T, C1);
-            C2 = fma2(mul2(f2(c.z), ae), T, C2);
-            T = make_float2(act0 ? test_T.x : T.x, act1 ? test_T.y : T.y);
-            const uint32_t idx = (uint32_t)(base + jj + 1);
-            lc0 = act0 ? idx : lc0;
-            lc1 = act1 ? idx : lc1;
-          }
-        }
-      }
-      warp_done = __all_sync(kFullMask, done0 && done1);
-    }
-  }
+  float2 T, C0, C1, C2;
+  uint32_t lc0, lc1;
+  forward_pass<kBatch, kWrap, true>(job, src, patch, s_a, s_b, s_c, T, lc0, lc1, C0, C1, C2);
 
   const int64_t HW = (int64_t)job.H * job.W;
   const float Ts[2] = {T.x, T.y}, Cs[3][2] = {{C0.x, C0.y}, {C1.x, C1.y}, {C2.x, C2.y}};
@@ -98,8 +39,10 @@ __device__ __forceinline__ void blend_forward_tile(const TileJob& job, const Ble
   for (int i = 0; i < 2; ++i) {
     if (!patch.inside(i, job.W, job.H)) continue;
     const int64_t pix = patch.pixel(i, job.W);
-    job.final_T[pix] = Ts[i];
-    job.n_contrib[pix] = lcs[i];
+    if (job.final_T != nullptr) {  // stored unless the backward recomputes it
+      job.final_T[pix] = Ts[i];
+      job.n_contrib[pix] = lcs[i];
+    }
 #pragma unroll
     for (int ch = 0; ch < 3; ++ch) job.out_color[ch * HW + pix] = __fmaf_rn(Ts[i], job.bg[ch], Cs[ch][i]);
   }

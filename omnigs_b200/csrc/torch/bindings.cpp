@@ -5,6 +5,7 @@
 
 #include "gaussian_rasterizer.h"
 #include "omnigs_b200.h"
+#include "omnigs_settings.h"
 #include "rasterize_points.h"
 
 namespace {
@@ -44,4 +45,7 @@ PYBIND11_MODULE(TORCH_EXTENSION_NAME, m) {
         py::arg("viewmatrix"), py::arg("projmatrix"), py::arg("camera_type") = 1);
   m.def("rasterize", &rasterize, "GaussianRasterizerFunction::apply (autograd)");
   m.def("version", []() { return std::string(omnigs_version()); });
+  m.def("set_recompute_transmittance", &omnigs_torch_set_recompute_transmittance,
+        "transmittance checkpointing for the following forwards (omnigs_settings.h)");
+  m.def("recompute_transmittance", &omnigs_torch_recompute_transmittance);
 }

@@ -7,7 +7,8 @@
 //    copy; the one host wait reads num_rendered (which this API returns by value) once the
 //    binning has run, while the blend still runs, and only when the hint was too small is the
 //    binning stage resized and re-run;
-//  * gradient outputs are allocated uninitialised because the backward writes every element.
+//  * gradient outputs are allocated uninitialised because the backward writes every element;
+//  * optional transmittance checkpointing (omnigs_settings.h).
 #include "rasterize_points.h"
 
 #include <ATen/cuda/CUDAContext.h>
@@ -17,12 +18,14 @@
 #include <stdexcept>
 
 #include "omnigs_b200.h"
+#include "omnigs_settings.h"
 
 namespace {
 
 constexpr int kChannels = 3;  // NUM_CHANNELS, cuda_rasterizer/config.h:25
 
 std::atomic<int64_t> g_capacity_hint{0};
+std::atomic<int> g_forward_flags{0};  // OMNIGS_FLAG_* of the next forwards
 
 void check_rc(int rc, const char* what) {
   if (rc != OMNIGS_OK)
@@ -52,6 +55,9 @@ struct FloatIn {
 }
 
 }  // namespace
+
+void omnigs_torch_set_recompute_transmittance(bool on) { g_forward_flags.store(on ? OMNIGS_FLAG_RECOMPUTE_T : 0); }
+bool omnigs_torch_recompute_transmittance() { return (g_forward_flags.load() & OMNIGS_FLAG_RECOMPUTE_T) != 0; }
 
 std::tuple<int, torch::Tensor, torch::Tensor, torch::Tensor, torch::Tensor, torch::Tensor>
 RasterizeGaussiansCUDA(const torch::Tensor& background, const torch::Tensor& means3D,
@@ -107,9 +113,10 @@ RasterizeGaussiansCUDA(const torch::Tensor& background, const torch::Tensor& mea
     a.campos = cp.ptr;
     a.out_color = out_color.data_ptr<float>();
     a.radii = radii.data_ptr<int>();
+    a.flags = g_forward_flags.load();
 
     geomBuffer.resize_({(int64_t)omnigs_lonlat_geom_bytes(P)});
-    imgBuffer.resize_({(int64_t)omnigs_lonlat_image_bytes(W, H)});
+    imgBuffer.resize_({(int64_t)omnigs_lonlat_image_bytes_flags(W, H, a.flags)});
     const int64_t capacity = std::max<int64_t>(g_capacity_hint.load(), 4 * (int64_t)P);
     binningBuffer.resize_({(int64_t)omnigs_lonlat_binning_bytes(capacity)});
     auto s = reinterpret_cast<omnigs_stream_t>(stream);
@@ -200,6 +207,8 @@ RasterizeGaussiansBackwardCUDA(const torch::Tensor& background, const torch::Ten
     a.dL_dscales = dL_dscales.data_ptr<float>();
     a.dL_drotations = dL_drotations.data_ptr<float>();
     a.dL_dconic = nullptr;
+    // the forward's mode, from its image buffer: only the checkpointing layout is that small
+    a.flags = imageBuffer.numel() < (int64_t)omnigs_lonlat_image_bytes(W, H) ? OMNIGS_FLAG_RECOMPUTE_T : 0;
     // The geometry buffer holds the per-splat gradient accumulators, so it is written here.
     torch::Tensor geom = geomBuffer;
     check_rc(omnigs_lonlat_backward(&a, geom.data_ptr(), geom.numel(), binningBuffer.data_ptr(),

@@ -83,14 +83,17 @@ def _view_tensor(base: torch.Tensor, address: int, count: int, dtype) -> torch.T
 
 
 class LonlatState:
-    """State buffers for P Gaussians rendered at W x H with room for ``capacity`` instances."""
+    """State buffers for P Gaussians rendered at W x H with room for ``capacity`` instances.
+    ``recompute_T`` selects transmittance checkpointing (OMNIGS_FLAG_RECOMPUTE_T): no per-pixel
+    state is stored and the backward recomputes it."""
 
-    def __init__(self, P: int, W: int, H: int, capacity: int, device="cuda"):
+    def __init__(self, P: int, W: int, H: int, capacity: int, device="cuda", recompute_T: bool = False):
         self.P, self.W, self.H = P, W, H
         self.device = torch.device(device)
+        self.flags = capi.FLAG_RECOMPUTE_T if recompute_T else 0
         u8 = dict(dtype=torch.uint8, device=self.device)
         self.geom = torch.empty(capi.geom_bytes(P), **u8)
-        self.image = torch.empty(capi.image_bytes(W, H), **u8)
+        self.image = torch.empty(capi.image_bytes(W, H, self.flags), **u8)
         self.binning = torch.empty(capi.binning_bytes(capacity), **u8)
 
     @property
@@ -116,6 +119,7 @@ class LonlatState:
         a.campos = capi.ptr(cam.campos)
         a.out_color = capi.ptr(out_color)
         a.radii = capi.ptr(radii)
+        a.flags = self.flags
         return a
 
     def forward(self, g: GaussianTensors, cam: Camera, out_color: torch.Tensor, radii: torch.Tensor,
@@ -169,6 +173,7 @@ class LonlatState:
                  stream=None):
         a = capi.BackwardArgs()
         a.P, a.D, a.M, a.W, a.H, a.R = g.P, D, g.M, cam.width, cam.height, R
+        a.flags = self.flags
         a.background = capi.ptr(cam.background)
         a.means3D = capi.ptr(g.means3D)
         a.shs = capi.ptr(g.shs)
@@ -219,6 +224,7 @@ class LonlatState:
         return dict(tile_ids=tiles, point_list=point_list, keys=keys)
 
     def image_view(self) -> dict:
+        assert self.flags == 0, "no per-pixel state is stored with recompute_T"
         v = capi.ImageView()
         capi.check(capi.lib().omnigs_lonlat_image_view(self.image.data_ptr(), self.W, self.H,
                                                        ctypes.byref(v)), "image_view")
@@ -230,11 +236,12 @@ class LonlatState:
 
 
 def rasterize(g: GaussianTensors, cam: Camera, D: int = 3, scale_modifier: float = 1.0,
-              capacity: int | None = None, state: LonlatState | None = None):
+              capacity: int | None = None, state: LonlatState | None = None, recompute_T: bool = False):
     """One forward pass with exact sizing; returns (image, radii, num_rendered, state)."""
     dev = g.means3D.device
     if state is None:
-        state = LonlatState(g.P, cam.width, cam.height, capacity or max(1024, 4 * g.P), dev)
+        state = LonlatState(g.P, cam.width, cam.height, capacity or max(1024, 4 * g.P), dev,
+                            recompute_T=recompute_T)
     out = torch.empty(3, cam.height, cam.width, dtype=torch.float32, device=dev)
     radii = torch.empty(g.P, dtype=torch.int32, device=dev)
     state.forward(g, cam, out, radii, D, scale_modifier)

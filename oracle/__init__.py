@@ -120,6 +120,25 @@ def binning(W, H, radii, means2D, depths, tiles_touched, f32: bool, seam_wrap: b
     return dict(num_rendered=R, keys=keys, point_list=vals, ranges=ranges)
 
 
+def binning_rows(W, H, radii, means2D, depths, row_lo, row_hi):
+    """FP64 binning restricted to tile rows [row_lo, row_hi): keys, point list and ranges of those
+    rows as the full FP64 binning has them; every other tile's range stays empty."""
+    radii = np.ascontiguousarray(radii, np.int32)
+    m2 = np.ascontiguousarray(means2D, np.float64)
+    d = np.ascontiguousarray(depths, np.float64)
+    P = radii.shape[0]
+    counts = np.zeros(P, np.uint32)
+    lib().oracle_tiles_in_rows_f64(P, W, H, _p(radii, P_i32), _p(m2, P_f64), row_lo, row_hi, _p(counts, P_u32))
+    R = int(counts.sum(dtype=np.int64))
+    gx, gy = (W + TILE - 1) // TILE, (H + TILE - 1) // TILE
+    keys = np.zeros(R, np.uint64)
+    vals = np.zeros(R, np.uint32)
+    ranges = np.zeros((gx * gy, 2), np.uint32)
+    lib().oracle_binning_f64_rows(P, W, H, _p(radii, P_i32), _p(m2, P_f64), _p(d, P_f64), _p(counts, P_u32),
+                                  row_lo, row_hi, _p(keys, P_u64), _p(vals, P_u32), _p(ranges, P_u32))
+    return dict(num_rendered=R, keys=keys, point_list=vals, ranges=ranges)
+
+
 def render_forward(W, H, ranges, point_list, means2D, conic_opacity, rgb, bg, nthreads=None,
                    seam_wrap=False):
     """Forward blend; ``seam_wrap`` measures x offsets to the splat copy nearest each pixel."""

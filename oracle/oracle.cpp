@@ -383,7 +383,7 @@ namespace {
 template <class T>
 void binning_impl(int P, int W, int H, const int* radii, const T* means2D, const float* depth32,
                   const uint32_t* tiles_touched, uint64_t* keys_out, uint32_t* vals_out,
-                  uint32_t* ranges, bool seam_wrap) {
+                  uint32_t* ranges, bool seam_wrap, int row_lo = 0, int row_hi = 1 << 30) {
   const int gx = (W + kTile - 1) / kTile, gy = (H + kTile - 1) / kTile;
   const int64_t tiles = (int64_t)gx * gy;
   std::vector<uint64_t> offs(P + 1, 0);
@@ -399,7 +399,7 @@ void binning_impl(int P, int W, int H, const int* radii, const T* means2D, const
     uint64_t off = offs[i];
     uint32_t dbits;
     std::memcpy(&dbits, &depth32[i], 4);
-    for (int y = rmin[1]; y < rmax[1]; ++y)
+    for (int y = std::max(rmin[1], row_lo); y < std::min(rmax[1], row_hi); ++y)
       for (int x = rmin[0]; x < rmax[0]; ++x) {
         const int col = ((x % gx) + gx) % gx;  // x itself unless the seam wraps
         uint64_t key = (uint32_t)(y * gx + col);
@@ -488,6 +488,33 @@ void oracle_binning_f64(int P, int W, int H, const int* radii, const double* mea
                         const double* depths, const uint32_t* tiles_touched, uint64_t* keys,
                         uint32_t* vals, uint32_t* ranges) {
   oracle_binning_f64_seam(P, W, H, radii, means2D, depths, tiles_touched, keys, vals, ranges, 0);
+}
+
+// Per-Gaussian instance counts restricted to tile rows [row_lo, row_hi) of the FP64 rects (for
+// oracle_binning_f64_rows).
+void oracle_tiles_in_rows_f64(int P, int W, int H, const int* radii, const double* means2D, int row_lo, int row_hi,
+                              uint32_t* counts) {
+  const int gx = (W + kTile - 1) / kTile, gy = (H + kTile - 1) / kTile;
+  for (int i = 0; i < P; ++i) {
+    counts[i] = 0;
+    if (!(radii[i] > 0)) continue;
+    int rmin[2], rmax[2];
+    get_rect<double>(means2D[2 * i], means2D[2 * i + 1], radii[i], gx, gy, rmin, rmax);
+    const int rows = std::min(rmax[1], row_hi) - std::max(rmin[1], row_lo);
+    if (rows > 0) counts[i] = (uint32_t)(rows * (rmax[0] - rmin[0]));
+  }
+}
+
+// Binning of the FP64 pipeline restricted to tile rows [row_lo, row_hi): the instances, sorted
+// list and ranges of those rows exactly as the full binning has them (other tiles stay empty),
+// for checking rows of a scene too large to bin whole on the CPU.  counts from
+// oracle_tiles_in_rows_f64.
+void oracle_binning_f64_rows(int P, int W, int H, const int* radii, const double* means2D, const double* depths,
+                             const uint32_t* counts, int row_lo, int row_hi, uint64_t* keys, uint32_t* vals,
+                             uint32_t* ranges) {
+  std::vector<float> d32(P);
+  for (int i = 0; i < P; ++i) d32[i] = (float)depths[i];
+  binning_impl<double>(P, W, H, radii, means2D, d32.data(), counts, keys, vals, ranges, false, row_lo, row_hi);
 }
 
 // Forward blend, forward.cu:346-467.  out_color [3,H,W], final_T [H*W], n_contrib [H*W].

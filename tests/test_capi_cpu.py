@@ -62,6 +62,7 @@ def _fake_args(**over):
     (dict(cov3D_precomp=0x10000), 1),             # both scale/rotation and cov3D
     (dict(rotations=None), 1),                    # half of the scale/rotation pair
     (dict(radii=None), 1),
+    (dict(flags=2), 1),                           # an unknown OMNIGS_FLAG_* bit
 ])
 def test_forward_argument_validation_precedes_device_work(over, code):
     a = _fake_args(**over)
@@ -97,7 +98,7 @@ def test_backward_rejects_capacity_mismatch():
     a.P, a.D, a.M, a.W, a.H, a.R = 10, 3, 16, 64, 32, 1000
     for f, _ in capi.BackwardArgs._fields_:
         if f not in ("P", "D", "M", "W", "H", "R", "scale_modifier", "colors_precomp",
-                     "cov3D_precomp", "dL_dconic"):
+                     "cov3D_precomp", "dL_dconic", "flags"):
             setattr(a, f, 0x10000)
     small = capi.binning_bytes(100)
     rc = capi.lib().omnigs_lonlat_backward(ctypes.byref(a), 0x10000, capi.geom_bytes(10), 0x10000,
@@ -283,3 +284,11 @@ def test_batch_tile_sort_runs_per_view_when_it_saves_a_pass(sizes, P, passes):
     sv = capi.BatchStateView()
     assert capi.lib().omnigs_batch_state_view(ctypes.c_void_p(0x10000), P, V, W, H, ctypes.byref(sv)) == 0
     assert sv.tile_passes == passes
+
+
+def test_checkpointing_image_buffer_holds_only_tile_ranges():
+    W, H = 2048, 1024
+    full, ckpt = capi.image_bytes(W, H), capi.image_bytes(W, H, capi.FLAG_RECOMPUTE_T)
+    tiles = (W // 16) * (H // 16)
+    assert ckpt == 8 * tiles
+    assert full - ckpt == 8 * W * H

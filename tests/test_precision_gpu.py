@@ -87,3 +87,58 @@ def test_precision_mode_against_fp64_oracle(cuda):
         assert report["precision"]["grad_l2_rel"][k] <= 1.1 * report["fp32"]["grad_l2_rel"][k] + 1e-6, k
     assert report["precision"]["psnr_vs_oracle_db"] >= report["fp32"]["psnr_vs_oracle_db"] - 0.05
     assert report["bf16_storage_psnr_db"] > 40.0
+
+
+def test_precision_configuration_full_size_rows(cuda):
+    """The precision configuration at its stated size: 6M Gaussians (30 % beyond 80 deg latitude),
+    one 4096x2048 view.  The whole FP64 pipeline does not fit a CPU budget at this size (943M
+    instances), so the oracle bins and blends three bands of tile rows exactly as its full binning
+    would (oracle.binning_rows: the pole row, a row near 80 deg, two equator rows) and the images
+    are compared there, against the oracle fed FP32 SH and against the oracle fed the bf16-rounded
+    SH the precision mode stores:
+      fp32      -- the single-view path with FP32 SH, against the FP32-SH oracle;
+      precision -- the batched path with BF16 SH and FP64 pole covariance, against both oracles
+                   (the FP32-SH comparison includes the cost of BF16 storage itself)."""
+    P, W, H = 6_000_000, 4096, 2048
+    g = scenes.make_gaussians(P, seed=4, pole_fraction=0.3)
+    view = scenes.identity_view(W, H)
+    gt = lonlat.GaussianTensors.from_numpy(g)
+    cam = lonlat.Camera.from_view(view)
+    img32 = helpers.to_np(lonlat.rasterize(gt, cam)[0])
+    gtb = lonlat.GaussianTensors(means3D=gt.means3D, opacities=gt.opacities, shs=gt.shs.to(torch.bfloat16),
+                                 scales=gt.scales, rotations=gt.rotations)
+    images, _, state = batch.render_batch(gtb, batch.BatchCameras.from_views([view]), fp64_poles=True)
+    imgp = helpers.to_np(images[0])
+    del state, images, gtb, gt
+    torch.cuda.empty_cache()
+
+    bg = np.zeros(3, np.float32)
+    pre32 = oracle.preprocess(g.means3D, g.scales, g.rotations, g.opacities, g.shs, view.viewmatrix,
+                              view.campos, W, H)
+    rgb16 = oracle.preprocess(g.means3D, g.scales, g.rotations, g.opacities, _bf16_round(g.shs),
+                              view.viewmatrix, view.campos, W, H)["rgb"]
+    report = {}
+    errs = {k: [] for k in ("fp32_vs_fp32sh", "precision_vs_bf16sh", "precision_vs_fp32sh")}
+    for name, (lo, hi) in (("pole", (0, 1)), ("lat80", (8, 9)), ("equator", (63, 65))):
+        b = oracle.binning_rows(W, H, pre32["radii"], pre32["means2D"], pre32["depths"], lo, hi)
+        rows = slice(16 * lo, 16 * hi)
+        ref32 = oracle.render_forward(W, H, b["ranges"], b["point_list"], pre32["means2D"],
+                                      pre32["conic_opacity"], pre32["rgb"], bg)["image"][:, rows]
+        ref16 = oracle.render_forward(W, H, b["ranges"], b["point_list"], pre32["means2D"],
+                                      pre32["conic_opacity"], rgb16, bg)["image"][:, rows]
+        band = {"instances": int(b["num_rendered"])}
+        for key, img, ref in (("fp32_vs_fp32sh", img32, ref32), ("precision_vs_bf16sh", imgp, ref16),
+                              ("precision_vs_fp32sh", imgp, ref32)):
+            d = np.abs(img[:, rows] - ref)
+            errs[key].append(d)
+            band[key] = {"max_abs": float(d.max()), "mean_abs": float(d.mean()), "psnr_db": _psnr(img[:, rows], ref)}
+        report[name] = band
+    for key, ds in errs.items():
+        d = np.concatenate([x.ravel() for x in ds])
+        mse = float((d.astype(np.float64) ** 2).mean())
+        report[key] = {"max_abs": float(d.max()), "mean_abs": float(d.mean()),
+                       "psnr_db": float("inf") if mse == 0 else 10 * np.log10(1.0 / mse)}
+    print("precision report (6M, 4096x2048, row bands):", json.dumps(report))
+    assert report["fp32_vs_fp32sh"]["psnr_db"] > 80.0, report
+    assert report["precision_vs_bf16sh"]["psnr_db"] > 80.0, report
+    assert report["precision_vs_fp32sh"]["psnr_db"] > 40.0, report
