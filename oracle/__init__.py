@@ -141,7 +141,8 @@ def binning_rows(W, H, radii, means2D, depths, row_lo, row_hi):
 
 def render_forward(W, H, ranges, point_list, means2D, conic_opacity, rgb, bg, nthreads=None,
                    seam_wrap=False):
-    """Forward blend; ``seam_wrap`` measures x offsets to the splat copy nearest each pixel."""
+    """Forward blend; ``seam_wrap`` measures x offsets to the splat copy nearest the centre of
+    each pixel's 8-column block."""
     ranges = np.ascontiguousarray(ranges, np.uint32)
     point_list = np.ascontiguousarray(point_list, np.uint32)
     means2D = np.ascontiguousarray(means2D, np.float64)

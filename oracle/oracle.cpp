@@ -169,9 +169,14 @@ inline void tile_rect(bool seam_wrap, T px, T py, int max_radius, int gx, int gy
 
 // x offset of a splat centre from a pixel column: the plain difference (the reference), or in
 // seam-wrapping mode the difference to the centre's copy (shifted by a multiple of the image
-// width) nearest the pixel.
+// width) nearest the centre of the pixel's block of 8 columns (columns 8k .. 8k + 7, centre
+// 8k + 3.5).  The mode defines the copy per 8-column block, not per pixel: a splat wider than
+// half the image reaches a block's pixels from one copy only, the one nearest the block.
 inline double seam_dx(bool seam_wrap, double mx, double px, int W) {
-  if (seam_wrap) mx -= W * std::nearbyint((mx - px) / W);
+  if (seam_wrap) {
+    const double block_centre = std::floor(px / 8.0) * 8.0 + 3.5;
+    mx -= W * std::nearbyint((mx - block_centre) / W);
+  }
   return mx - px;
 }
 
@@ -518,7 +523,7 @@ void oracle_binning_f64_rows(int P, int W, int H, const int* radii, const double
 }
 
 // Forward blend, forward.cu:346-467.  out_color [3,H,W], final_T [H*W], n_contrib [H*W].
-// seam_wrap != 0: x offsets to the splat's copy nearest the pixel (seam_dx).
+// seam_wrap != 0: x offsets to the splat's copy nearest the pixel's 8-column block (seam_dx).
 void oracle_render_forward_seam(int W, int H, const uint32_t* ranges, const uint32_t* point_list,
                                 const double* means2D, const double* conic_opacity, const double* rgb,
                                 const float* bg, double* out_color, double* final_T,
@@ -567,7 +572,7 @@ void oracle_render_forward(int W, int H, const uint32_t* ranges, const uint32_t*
 // Gaussian in instance order, which makes the oracle deterministic.
 // Outputs (zeroed here): dL_dmean2D [P,3], dL_dconic [P,4] (x, y, -, w), dL_dopacity [P],
 // dL_dcolor [P,3].
-// seam_wrap != 0: x offsets to the splat's copy nearest the pixel (seam_dx); the offset's
+// seam_wrap != 0: x offsets to the splat's copy nearest the pixel's 8-column block (seam_dx); the offset's
 // derivative with respect to the centre is 1 for every copy, so the formulas are unchanged.
 void oracle_render_backward_seam(int P, int W, int H, const uint32_t* ranges, const uint32_t* point_list,
                                  int64_t R, const double* means2D, const double* conic_opacity,
