@@ -317,7 +317,7 @@ int omnigs_batch_read_status(const void* state, int V, int64_t* num_rendered, in
  * max_spins polls, sets OMNIGS_STATUS_LOOKBACK and the kernel finishes.  Then waits for `stream`,
  * returns the status word in *status and OMNIGS_ERR_DEVICE when a bit other than capacity is set.
  * The buffers hold no valid forward afterwards; a following omnigs_lonlat_forward resets them.
- * Needs P > 256.  For tests: real passes never skip a tile. */
+ * Needs P > 1024.  For tests: real passes never skip a tile. */
 int omnigs_debug_lookback_timeout(const OmnigsLonlatForwardArgs* args, void* geom, size_t geom_bytes,
                                   void* binning, size_t binning_bytes, void* image, size_t image_bytes,
                                   int max_spins, uint32_t* status, omnigs_stream_t stream);

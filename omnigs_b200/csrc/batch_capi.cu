@@ -31,8 +31,8 @@ struct BatchPlan {
 // The tile sort of a batch.  Each view's instances leave the duplicate pass contiguous (view after
 // view), so the sort can run per view on view-local tile ids, which need fewer digits than the
 // batch's global ids when the views together hold more than 2^k tiles and the largest alone fewer.
-// Per view, each segment has its own digit histograms (counted by the duplicate pass, which needs
-// P >= kScanBlock so that one of its blocks spans at most two views) and its own look-back chain.
+// Per view, each segment has its own digit histograms (counted by the duplicate pass's emission)
+// and its own look-back chain.
 struct BatchTileSort {
   TileDigits digits;
   bool per_view;
@@ -43,7 +43,7 @@ BatchTileSort batch_tile_sort(const BatchPlan& plan) {
   int64_t max_view_tiles = 1;
   for (int v = 0; v < plan.V; ++v) max_view_tiles = std::max(max_view_tiles, plan.view_tiles[v]);
   const TileDigits local = TileDigits::from_tiles((uint32_t)max_view_tiles);
-  const bool per_view = plan.V > 1 && plan.P >= kScanBlock && local.passes < global.passes;
+  const bool per_view = plan.V > 1 && local.passes < global.passes;
   return {per_view ? local : global, per_view};
 }
 
@@ -280,6 +280,9 @@ int omnigs_batch_render(const OmnigsBatchArgs* a, void* state, size_t state_byte
   d.tkeys = tkeys[0];
   d.tvals = tvals[0];
   d.scan_state = at<unsigned long long>(state, L.dup_scan);
+  d.incl = dkeys[0];  // free once the last depth pass has read it (the sorted keys are in dkeys[1])
+  d.emit_first = at<uint32_t>(binning, BL.emit_first);
+  d.emit_last = at<uint32_t>(binning, BL.emit_last);
   d.capacity = capacity;
   d.hdr = hdr;
   d.seam_wrap = a->seam_wrap;

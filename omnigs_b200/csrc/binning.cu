@@ -8,9 +8,9 @@
 // same order is produced here with far fewer passes over the instances:
 //  1. depth sort: a stable LSD radix sort (4 onesweep passes of 8 bits) of the P Gaussians by the
 //     bits of their depth, i.e. the order (depth bits, index);
-//  2. duplicate: instances are emitted walking the Gaussians in that order, each block scanning
-//     its Gaussians' tile counts and joining a decoupled look-back for its output offset, and
-//     counting the digits of the keys it writes for the tile sort;
+//  2. duplicate: a scan of the Gaussians' tile counts in that order (decoupled look-back), then
+//     a load-balanced emission of the instances in that order (every block writes the same number
+//     of instances), counting the digits of the keys it writes for the tile sort;
 //  3. tile sort: a stable LSD radix sort (2 onesweep passes) of the instances by tile id only
 //     (for a batch of views, per view on view-local tile ids when those need fewer passes than
 //     the batch's global ids: each view's instances are contiguous after step 2).
@@ -102,6 +102,7 @@ __global__ void __launch_bounds__(256) histogram_kernel(const __grid_constant__ 
 }
 
 // ---------------------------------------------------------------- onesweep pass ---------------
+template <int kTile>
 struct SortSmem {
   uint32_t warp_hist[kSortThreads / 32][kRadix];
   uint32_t block_excl[kRadix];
@@ -109,8 +110,8 @@ struct SortSmem {
   uint32_t scan_tmp[kSortThreads / 32];
   uint32_t tile;
   uint32_t pad[3];
-  uint32_t keys[kSortTile];
-  uint32_t vals[kSortTile];
+  uint32_t keys[kTile];
+  uint32_t vals[kTile];
   // the block's segment as thread 0 resolved it (variable segments): index (num_segs: none), item
   // count, tile within the segment, first item, key base
   uint32_t seg, seg_n, seg_tile, seg_first, seg_key_base;
@@ -156,13 +157,18 @@ __device__ __forceinline__ uint32_t block_exclusive_scan(uint32_t v, uint32_t* s
 // with a 128-byte one.
 static_assert(sizeof(OnesweepParams) <= 128, "keep the onesweep parameter block at 128 bytes or less");
 
+// Tiles of kSortTile keys, 16 per thread.  Measured on a B200: 1024-key tiles (4 per thread, five
+// blocks per SM) made the depth passes over 1M Gaussians slower, 22 -> 30 us each (4x the blocks,
+// look-back chains and per-tile scans), so every pass uses the 4096-key tiles.
 template <bool kVarSeg>
 __global__ void __launch_bounds__(kSortThreads, 3) onesweep_kernel(OnesweepParams p) {
-  __shared__ SortSmem sm;
+  constexpr int kItems = kSortItems;
+  constexpr int kTile = kSortTile;
+  __shared__ SortSmem<kTile> sm;
   uint32_t n = 0, tiles_per_seg = 1, ntiles = 0;
   if (!kVarSeg) {
     n = p.seg_len ? p.seg_len : item_count(p.count_hdr, p.n_host, p.capacity);
-    tiles_per_seg = (n + kSortTile - 1) / kSortTile;
+    tiles_per_seg = (n + kTile - 1) / kTile;
     ntiles = tiles_per_seg * (p.seg_len ? p.num_segs : 1u);
   }
   if (threadIdx.x == 0) {
@@ -174,7 +180,7 @@ __global__ void __launch_bounds__(kSortThreads, 3) onesweep_kernel(OnesweepParam
       sm.seg = p.num_segs;
       for (uint32_t sg = 0; sg < p.num_segs; ++sg) {
         const uint32_t ns = fit ? (uint32_t)p.seg_counts[sg] : 0u;
-        const uint32_t ts = (ns + kSortTile - 1) / kSortTile;
+        const uint32_t ts = (ns + kTile - 1) / kTile;
         if (t < first_tile + ts) {
           sm.seg = sg;
           sm.seg_n = ns;
@@ -217,15 +223,15 @@ __global__ void __launch_bounds__(kSortThreads, 3) onesweep_kernel(OnesweepParam
   const int shift = p.shift;
 
   // load the whole tile first (independent loads in flight), then rank
-  uint32_t key[kSortItems], val[kSortItems];
-  const uint32_t tile_base = tile * kSortTile + warp * (kSortItems * 32) + lane;
+  uint32_t key[kItems], val[kItems];
+  const uint32_t tile_base = tile * kTile + warp * (kItems * 32) + lane;
 #pragma unroll
-  for (int k = 0; k < kSortItems; ++k) {
+  for (int k = 0; k < kItems; ++k) {
     const uint32_t idx = tile_base + k * 32;
     key[k] = idx < n ? keys_in[idx] : 0xffffffffu;
   }
 #pragma unroll
-  for (int k = 0; k < kSortItems; ++k) {
+  for (int k = 0; k < kItems; ++k) {
     const uint32_t idx = tile_base + k * 32;
     val[k] = idx < n ? (vals_in ? vals_in[idx] : (uint32_t)(seg_base + idx)) : 0u;
   }
@@ -233,9 +239,9 @@ __global__ void __launch_bounds__(kSortThreads, 3) onesweep_kernel(OnesweepParam
   uint32_t unused;
   sm.global_base[threadIdx.x] = block_exclusive_scan(hist[threadIdx.x], sm.scan_tmp, unused);
 
-  uint32_t rank[kSortItems];
+  uint32_t rank[kItems];
 #pragma unroll
-  for (int k = 0; k < kSortItems; ++k) {
+  for (int k = 0; k < kItems; ++k) {
     const bool valid = tile_base + k * 32 < n;
     const uint32_t digit = (key[k] >> shift) & mask;
     const unsigned peers = __match_any_sync(kFullMask, valid ? digit : (0x10000u | lane));
@@ -308,11 +314,11 @@ __global__ void __launch_bounds__(kSortThreads, 3) onesweep_kernel(OnesweepParam
 
   // reorder the tile in shared memory by digit
 #pragma unroll
-  for (int k = 0; k < kSortItems; ++k) {
+  for (int k = 0; k < kItems; ++k) {
     if (rank[k] != 0xffffffffu) {
       const uint32_t digit = (key[k] >> shift) & mask;
       const uint32_t pos = sm.block_excl[digit] + sm.warp_hist[warp][digit] + rank[k];
-      if (pos < (uint32_t)kSortTile) {  // always true: ranks are consistent within the block
+      if (pos < (uint32_t)kTile) {  // always true: ranks are consistent within the block
         sm.keys[pos] = key[k];
         sm.vals[pos] = val[k];
       }
@@ -333,63 +339,90 @@ __global__ void __launch_bounds__(kSortThreads, 3) onesweep_kernel(OnesweepParam
 }
 
 // ---------------------------------------------------------------- duplicate -------------------
-// duplicateWithKeys over the depth-sorted Gaussians, fused with the scan of their tile counts and
-// with the digit histograms of the tile sort that follows.
-// Block b takes sorted positions [256 b, 256 b + 256); its output offset comes from a block scan
-// plus a decoupled look-back over the preceding blocks.  Each warp then writes the instances of
-// its 32 Gaussians (one contiguous span) 32 at a time: a 5-step shuffle search finds each
-// instance's Gaussian, so a splat covering hundreds of tiles does not serialise one thread.
+// duplicateWithKeys (rasterizer_impl.cu:94-140) over the depth-sorted Gaussians, in two kernels:
+//  1. instance_scan_kernel: the inclusive scan of the Gaussians' tile counts in depth order (block
+//     b takes sorted positions [1024 b, 1024 b + 1024), four per thread: block scan plus a
+//     decoupled look-back over the preceding blocks), written to p.incl; every Gaussian whose
+//     instances hold the first or last instance of an emit block (kEmitBlock instances) records
+//     its position there (p.emit_first / p.emit_last);
+//  2. instance_emit_kernel: block b writes instances [2048 b, 2048 b + 2048) of the list: every
+//     block does the same amount of work however the instances are spread over the Gaussians
+//     (the nearest splats, first in depth order, cover thousands of tiles each).  It stages the
+//     offsets and tile rects of its Gaussians in shared memory, each thread finds its instances'
+//     Gaussians by binary search there, and counts the digit histograms of the tile sort that
+//     follows while writing the keys.
+// One kernel doing both measured ~150 us at 400k and 1M Gaussians alike: a block's warps each
+// emitted their own Gaussians' instances, so a block held its SM slots until its busiest warp was
+// done (62 % of the stall samples were barrier waits).
+
+// Tile rect of record `rec` (view `view`) in the duplicate's terms: instance count, rect width,
+// first column, tile-id pitch and the id of the rect's first row (view-local when per view).
+struct RecordRect {
+  uint32_t count, row_origin;
+  int pitch, width, col0;
+};
+
 template <bool kPerView>
-__global__ void __launch_bounds__(kScanBlock) duplicate_kernel(const __grid_constant__ DuplicateParams p) {
+__device__ __forceinline__ RecordRect record_rect(const DuplicateParams& p, uint32_t rec, uint32_t view) {
+  RecordRect r;
+  r.count = 0;
+  r.row_origin = 0;
+  r.pitch = 1;
+  r.width = 1;
+  r.col0 = 0;
+  const int radius = (rec - view * (uint32_t)p.P < (uint32_t)p.P) ? p.radii[rec] : 0;
+  if (radius > 0) {
+    const float4 a = p.splat[2 * rec];
+    const int gx = p.gx[view];
+    int2 rmin, rmax;
+    if (p.seam_wrap)
+      tile_rect_cyclic(make_float2(a.x, a.y), radius, gx, p.gy[view], rmin, rmax);
+    else
+      tile_rect(make_float2(a.x, a.y), radius, gx, p.gy[view], rmin, rmax);
+    r.width = rmax.x - rmin.x;
+    r.count = (uint32_t)r.width * (uint32_t)(rmax.y - rmin.y);
+    if (r.count == 0) r.width = 1;
+    r.pitch = gx;
+    r.col0 = rmin.x;
+    // per-view counting writes view-local tile ids (the tile sort restores the global ids)
+    r.row_origin = (kPerView ? 0u : p.tile_base[view]) + (uint32_t)rmin.y * (uint32_t)gx;
+  }
+  return r;
+}
+
+__device__ __forceinline__ uint32_t record_view(const DuplicateParams& p, uint32_t i) {
+  return (p.V == 1) ? 0u : i / (uint32_t)p.P;  // the depth order keeps records in their view
+}
+
+constexpr int kScanItems = kScanTile / kScanBlock;  // Gaussians per scan thread
+
+template <bool kPerView>
+__global__ void __launch_bounds__(kScanBlock) instance_scan_kernel(const __grid_constant__ DuplicateParams p) {
   __shared__ uint32_t s_tile;
   __shared__ uint32_t s_warp[kScanBlock / 32];
   __shared__ unsigned long long s_excl;
-  // digit counts of the tile sort: [slot][pass][digit], slot = view - (the block's first view)
-  // when counted per view (a block then spans at most two views), else one slot
-  constexpr int kHistSlot = kTilePasses * kRadix;
-  constexpr int kSlots = kPerView ? 2 : 1;
-  __shared__ uint32_t s_hist[kSlots * kHistSlot];
   if (!instances_fit(p.hdr, p.capacity)) {
     if (blockIdx.x == 0 && threadIdx.x == 0) atomicOr(&p.hdr->status, kStatusCapacity);
     return;
   }
   if (kPerView && blockIdx.x == 0 && threadIdx.x < p.V) p.key_base_out[threadIdx.x] = p.tile_base[threadIdx.x];
   if (threadIdx.x == 0) s_tile = atomicAdd(&p.hdr->dup_tile_counter, 1u) + p.skip_tiles;
-  for (int k = threadIdx.x; k < kSlots * kHistSlot; k += kScanBlock) s_hist[k] = 0;
   __syncthreads();
   const uint32_t tile = s_tile;
   const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
   const uint32_t items = (uint32_t)p.P * (uint32_t)p.V;
-  const uint32_t i = tile * kScanBlock + threadIdx.x;
-  const uint32_t view0 = (p.V == 1) ? 0u : (tile * kScanBlock) / (uint32_t)p.P;
-  uint32_t count = 0, g = 0, row_origin = 0, my_view = view0;
-  int pitch = 1, width = 1, col0 = 0;
-  float inv_width = 1.f;
-  if (i < items) {
-    const uint32_t view = (p.V == 1) ? 0u : i / (uint32_t)p.P;  // the order keeps records in their view
-    my_view = view;
-    g = p.order[i];
-    const int radius = (g - view * (uint32_t)p.P < (uint32_t)p.P) ? p.radii[g] : 0;
-    if (radius > 0) {
-      const float4 a = p.splat[2 * g];
-      const int gx = p.gx[view];
-      int2 rmin, rmax;
-      if (p.seam_wrap)
-        tile_rect_cyclic(make_float2(a.x, a.y), radius, gx, p.gy[view], rmin, rmax);
-      else
-        tile_rect(make_float2(a.x, a.y), radius, gx, p.gy[view], rmin, rmax);
-      width = rmax.x - rmin.x;
-      count = (uint32_t)width * (uint32_t)(rmax.y - rmin.y);
-      if (count == 0) width = 1;
-      inv_width = 1.f / (float)width;
-      pitch = gx;
-      col0 = rmin.x;
-      // per-view counting writes view-local tile ids (the tile sort restores the global ids)
-      row_origin = (kPerView ? 0u : p.tile_base[view]) + (uint32_t)rmin.y * (uint32_t)gx;
-    }
+  const uint32_t i0 = tile * (uint32_t)kScanTile + threadIdx.x * (uint32_t)kScanItems;
+  uint32_t cnt[kScanItems];
+#pragma unroll
+  for (int u = 0; u < kScanItems; ++u) {
+    const uint32_t i = i0 + u;
+    cnt[u] = i < items ? record_rect<kPerView>(p, p.order[i], record_view(p, i)).count : 0u;
   }
-  // block inclusive scan of the counts
-  uint32_t v = count;
+  uint32_t thread_total = 0;
+#pragma unroll
+  for (int u = 0; u < kScanItems; ++u) thread_total += cnt[u];
+  // block inclusive scan of the thread totals
+  uint32_t v = thread_total;
 #pragma unroll
   for (int o = 1; o < 32; o <<= 1) {
     const uint32_t n = __shfl_up_sync(kFullMask, v, o);
@@ -407,7 +440,7 @@ __global__ void __launch_bounds__(kScanBlock) duplicate_kernel(const __grid_cons
     if (lane < kScanBlock / 32) s_warp[lane] = w;
   }
   __syncthreads();
-  const uint32_t incl_local = v + (warp > 0 ? s_warp[warp - 1] : 0u);
+  const uint32_t thread_excl = v - thread_total + (warp > 0 ? s_warp[warp - 1] : 0u);
   const unsigned long long block_total = s_warp[kScanBlock / 32 - 1];
   // decoupled look-back across blocks (warp 0)
   if (warp == 0) {
@@ -455,64 +488,149 @@ __global__ void __launch_bounds__(kScanBlock) duplicate_kernel(const __grid_cons
     }
   }
   __syncthreads();
-  const uint32_t start = (uint32_t)(s_excl + incl_local - count);
-  const uint32_t last_tile = (items + kScanBlock - 1) / kScanBlock - 1u;
-  if (tile == last_tile && threadIdx.x == kScanBlock - 1 && s_excl + block_total != p.hdr->num_rendered64)
-    atomicOr(&p.hdr->status, kStatusInconsistent);
-
-  // emit this warp's instances
-  const uint32_t w_begin = __shfl_sync(kFullMask, start, 0);
-  const uint32_t w_end = __shfl_sync(kFullMask, start + count, 31);
-  const uint32_t limit = (uint32_t)min((long long)p.capacity, 0xffffffffll);
-  for (uint32_t o0 = w_begin; o0 < w_end; o0 += 32) {
-    const uint32_t o = o0 + lane;
-    int pos = 0;
+  const unsigned long long R = p.hdr->num_rendered64;
+  const uint32_t nblocks = (uint32_t)((R + kEmitBlock - 1) / kEmitBlock);  // emit blocks (R fits the capacity)
+  unsigned long long incl = s_excl + thread_excl;
 #pragma unroll
-    for (int step = 16; step > 0; step >>= 1) {
-      const uint32_t s = __shfl_sync(kFullMask, start, pos + step);
-      if (s <= o) pos += step;
+  for (int u = 0; u < kScanItems; ++u) {
+    const uint32_t i = i0 + u;
+    const unsigned long long start = incl;
+    incl += cnt[u];
+    if (i >= items) continue;
+    p.incl[i] = (uint32_t)min(incl, 0xffffffffull);
+    if (cnt[u] == 0 || incl > R) continue;  // (past R only when the scan is inconsistent)
+    // the emit blocks whose first instance (b * kEmitBlock) lies in [start, incl)
+    for (unsigned long long b = (start + kEmitBlock - 1) / kEmitBlock; b * kEmitBlock < incl && b < nblocks; ++b)
+      p.emit_first[b] = i;
+    // ... and whose last instance (min((b + 1) kEmitBlock, R) - 1) does
+    for (unsigned long long b = start / kEmitBlock; b < nblocks && b * kEmitBlock < incl; ++b) {
+      const unsigned long long last = min((b + 1) * (unsigned long long)kEmitBlock, R) - 1;
+      if (last >= start && last < incl) p.emit_last[b] = i;
     }
-    const uint32_t o_start = __shfl_sync(kFullMask, start, pos);
-    const uint32_t o_origin = __shfl_sync(kFullMask, row_origin, pos);
-    const int o_pitch = __shfl_sync(kFullMask, pitch, pos);
-    const int o_width = __shfl_sync(kFullMask, width, pos);
-    const float o_inv = __shfl_sync(kFullMask, inv_width, pos);
-    const int o_col0 = __shfl_sync(kFullMask, col0, pos);
-    const uint32_t o_g = __shfl_sync(kFullMask, g, pos);
-    const bool ok = o < w_end && o < limit;
-    uint32_t key = 0;
+  }
+  const uint32_t last_tile = (items + kScanTile - 1) / kScanTile - 1u;
+  if (tile == last_tile && threadIdx.x == kScanBlock - 1 && s_excl + block_total != R)
+    atomicOr(&p.hdr->status, kStatusInconsistent);
+}
+
+constexpr int kEmitPerThread = kEmitBlock / kScanBlock;
+constexpr int kEmitStage = kEmitBlock + 1;  // Gaussians of a block staged in shared memory
+
+__device__ __forceinline__ float rcp_approx_f(float x) {
+  float r;
+  asm("rcp.approx.ftz.f32 %0, %1;" : "=f"(r) : "f"(x));
+  return r;
+}
+
+template <bool kPerView>
+__global__ void __launch_bounds__(kScanBlock) instance_emit_kernel(const __grid_constant__ DuplicateParams p) {
+  // digit counts of the tile sort: [slot][pass][digit], slot = view - (the block's first view)
+  // when counted per view; views past kSlots (a block spanning many small views) count directly
+  // into the global histogram
+  constexpr int kHistSlot = kTilePasses * kRadix;
+  constexpr int kSlots = kPerView ? 2 : 1;
+  __shared__ uint32_t s_hist[kSlots * kHistSlot];
+  // the block's Gaussians: inclusive offset, record, first row's tile id, first column | width,
+  // tile-id pitch | view
+  __shared__ uint32_t s_incl[kEmitStage], s_rec[kEmitStage], s_row[kEmitStage], s_cw[kEmitStage], s_pv[kEmitStage];
+  if (!instances_fit(p.hdr, p.capacity)) return;  // the scan kernel has flagged the overflow
+  const uint32_t R = p.hdr->num_rendered;
+  const uint32_t o_lo = blockIdx.x * (uint32_t)kEmitBlock;
+  if (o_lo >= R) return;
+  const uint32_t o_hi = min(R, o_lo + (uint32_t)kEmitBlock);  // exclusive (R <= capacity)
+  const int lane = threadIdx.x & 31;
+  const uint32_t items = (uint32_t)p.P * (uint32_t)p.V;
+  for (int k = threadIdx.x; k < kSlots * kHistSlot; k += kScanBlock) s_hist[k] = 0;
+  // (both clamped: after an inconsistent scan, which the status word reports, the entries may be
+  // stale; the reads stay in range)
+  const uint32_t g_first = min(p.emit_first[blockIdx.x], items - 1u);
+  const uint32_t g_last = min(p.emit_last[blockIdx.x], items - 1u);
+  const uint32_t n = g_last >= g_first ? g_last - g_first + 1u : 1u;
+  // Gaussians between g_first and g_last with no instances (culled views' records) can make the
+  // range longer than the block's instance count: then offsets and rects are read from global memory
+  const bool staged = n <= (uint32_t)kEmitStage;
+  if (staged)
+    for (uint32_t t = threadIdx.x; t < n; t += kScanBlock) {
+      const uint32_t i = g_first + t;
+      const uint32_t view = record_view(p, i);
+      const uint32_t rec = p.order[i];
+      const RecordRect r = record_rect<kPerView>(p, rec, view);
+      s_incl[t] = p.incl[i];
+      s_rec[t] = rec;
+      s_row[t] = r.row_origin;
+      s_cw[t] = ((uint32_t)r.col0 & 0xffffu) | ((uint32_t)r.width << 16);
+      s_pv[t] = (uint32_t)r.pitch | (view << 16);
+    }
+  __syncthreads();
+  const uint32_t* incl = staged ? s_incl : p.incl + g_first;
+  const uint32_t excl0 = g_first > 0 ? p.incl[g_first - 1] : 0u;
+  const uint32_t view0 = record_view(p, g_first);
+#pragma unroll 2
+  for (int k = 0; k < kEmitPerThread; ++k) {
+    const uint32_t o = o_lo + (uint32_t)(k * kScanBlock) + threadIdx.x;
+    const bool ok = o < o_hi;
+    uint32_t key = 0, view = view0;
     if (ok) {
-      const uint32_t local = o - o_start;
-      // local / width from the float reciprocal: local < 2^21 (a rect holds at most every tile of
-      // a view), so the truncated estimate is within one of the quotient; one step fixes it
-      uint32_t ry = (uint32_t)((float)local * o_inv);
-      int rem = (int)(local - ry * (uint32_t)o_width);
+      // j: the first of the block's Gaussians whose inclusive offset exceeds o
+      uint32_t lo = 0, hi = n - 1u;
+      while (lo < hi) {
+        const uint32_t mid = (lo + hi) >> 1;
+        if (incl[mid] > o)
+          hi = mid;
+        else
+          lo = mid + 1u;
+      }
+      const uint32_t start = lo > 0 ? incl[lo - 1] : excl0;
+      uint32_t rec, row_origin;
+      int col0, width, pitch;
+      if (staged) {
+        rec = s_rec[lo];
+        row_origin = s_row[lo];
+        const uint32_t cw = s_cw[lo], pv = s_pv[lo];
+        col0 = (int)(int16_t)(cw & 0xffffu);
+        width = (int)(cw >> 16);
+        pitch = (int)(pv & 0xffffu);
+        view = pv >> 16;
+      } else {
+        view = record_view(p, g_first + lo);
+        rec = p.order[g_first + lo];
+        const RecordRect r = record_rect<kPerView>(p, rec, view);
+        row_origin = r.row_origin;
+        col0 = r.col0;
+        width = r.width;
+        pitch = r.pitch;
+      }
+      const uint32_t local = o - start;
+      // local / width from an approximate reciprocal: local < 2^21 (a rect holds at most every
+      // tile of a view), so the truncated estimate is within one of the quotient; one step fixes it
+      uint32_t ry = (uint32_t)((float)local * rcp_approx_f((float)width));
+      int rem = (int)(local - ry * (uint32_t)width);
       if (rem < 0) {
         ry -= 1u;
-        rem += o_width;
-      } else if (rem >= o_width) {
+        rem += width;
+      } else if (rem >= width) {
         ry += 1u;
-        rem -= o_width;
+        rem -= width;
       }
-      int tx = o_col0 + rem;
-      if (tx < 0) tx += o_pitch;  // seam wrap: columns left of 0 or right of gx - 1
-      if (tx >= o_pitch) tx -= o_pitch;
-      key = o_origin + ry * (uint32_t)o_pitch + (uint32_t)tx;
+      int tx = col0 + rem;
+      if (tx < 0) tx += pitch;  // seam wrap: columns left of 0 or right of gx - 1
+      if (tx >= pitch) tx -= pitch;
+      key = row_origin + ry * (uint32_t)pitch + (uint32_t)tx;
       p.tkeys[o] = key;
-      p.tvals[o] = o_g;
+      p.tvals[o] = rec;
     }
     // digit histograms of the tile sort (the pass that would otherwise re-read every key)
-    const uint32_t slot = kPerView ? __shfl_sync(kFullMask, my_view, pos) - view0 : 0u;
-    // A block spans at most kSlots views when every view has at least kScanBlock Gaussians (the
-    // batched entry points require that); a slot past them is counted nowhere and flagged.
+    const uint32_t slot = kPerView ? view - view0 : 0u;
     const bool counted = ok && slot < (uint32_t)kSlots;
-    if (kPerView && __any_sync(kFullMask, ok && !counted) && lane == 0) atomicOr(&p.hdr->status, kStatusInconsistent);
     const unsigned live = __ballot_sync(kFullMask, counted);
 #pragma unroll
     for (int q = 0; q < kTilePasses; ++q)
-      if (q < p.hist_passes)
-        count_digit(s_hist, slot * kHistSlot + q * kRadix + ((key >> p.hist_shift[q]) & p.hist_mask[q]), counted,
-                    live, lane);
+      if (q < p.hist_passes) {
+        const uint32_t digit = (key >> p.hist_shift[q]) & p.hist_mask[q];
+        count_digit(s_hist, slot * kHistSlot + q * kRadix + digit, counted, live, lane);
+        if (kPerView && ok && !counted)
+          atomicAdd(&p.hist[(size_t)view * kHistSlot + q * kRadix + digit], 1u);
+      }
   }
   if (p.hist_passes == 0) return;
   __syncthreads();
@@ -578,14 +696,23 @@ void launch_onesweep(const OnesweepParams& p, int64_t max_items, cudaStream_t s)
 void launch_duplicate(const DuplicateParams& p, cudaStream_t s) {
   const int64_t items = (int64_t)p.P * p.V;
   if (items <= 0) return;
-  const int64_t tiles = (items + kScanBlock - 1) / kScanBlock;
+  const int64_t tiles = (items + kScanTile - 1) / kScanTile;
   if (tiles <= (int64_t)p.skip_tiles) return;
-  // one block per scan tile that is taken: block k takes tile skip_tiles + k
+  // scan: one block per scan tile that is taken (block k takes tile skip_tiles + k)
   const unsigned blocks = (unsigned)(tiles - p.skip_tiles);
   if (p.hist_per_view)
-    duplicate_kernel<true><<<blocks, kScanBlock, 0, s>>>(p);
+    instance_scan_kernel<true><<<blocks, kScanBlock, 0, s>>>(p);
   else
-    duplicate_kernel<false><<<blocks, kScanBlock, 0, s>>>(p);
+    instance_scan_kernel<false><<<blocks, kScanBlock, 0, s>>>(p);
+  // emit: one block per kEmitBlock instances the binning buffer can hold (blocks past the device's
+  // instance count return at once); a probe pass stops after the scan
+  if (p.skip_tiles != 0) return;
+  const int64_t eblocks = emit_blocks(std::min<int64_t>(p.capacity, 0xffffffffll));
+  if (eblocks <= 0) return;
+  if (p.hist_per_view)
+    instance_emit_kernel<true><<<(unsigned)eblocks, kScanBlock, 0, s>>>(p);
+  else
+    instance_emit_kernel<false><<<(unsigned)eblocks, kScanBlock, 0, s>>>(p);
 }
 
 void launch_ranges(const RangesParams& p, cudaStream_t s) {

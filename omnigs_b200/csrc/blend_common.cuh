@@ -143,8 +143,9 @@ __device__ __forceinline__ float2 splat_power2(const float4& a, const float4& b,
 }
 
 // Stages instances [base, base + cnt) of the tile's list (from the back when reverse: slot t holds
-// position base_hi - 1 - t, with base the exclusive upper end) into shared memory; s_c (colour) and
-// s_g (record index) may be NULL.
+// position base_hi - 1 - t, with base the exclusive upper end) into shared memory; the colour (s_c)
+// only with kColor, the record index only when s_g is not NULL.
+template <bool kColor = true>
 __device__ __forceinline__ void stage_batch(const BlendSource& src, uint32_t range_begin, int base, int cnt,
                                             bool reverse, float4* s_a, float4* s_b, float4* s_c,
                                             uint32_t* s_g) {
@@ -155,13 +156,13 @@ __device__ __forceinline__ void stage_batch(const BlendSource& src, uint32_t ran
       if (s_g) s_g[t] = g;
       s_a[t] = src.splat[2 * g];
       s_b[t] = src.splat[2 * g + 1];
-      if (s_c) s_c[t] = src.color[g];
+      if (kColor) s_c[t] = src.color[g];
     } else {  // unreachable for a consistent instance list; stage a splat that never contributes:
               // finite, unit conic, threshold -inf (no patch test hits), opacity 0 (alpha 0)
       if (s_g) s_g[t] = 0;
       s_a[t] = make_float4(0.f, 0.f, 1.f, 0.f);
       s_b[t] = make_float4(1.f, 0.f, -__int_as_float(0x7f800000), 1.f);
-      if (s_c) s_c[t] = make_float4(0.f, 0.f, 0.f, 0.f);
+      if (kColor) s_c[t] = make_float4(0.f, 0.f, 0.f, 0.f);
     }
   }
 }
@@ -189,8 +190,7 @@ __device__ __forceinline__ void forward_pass(const TileJob& job, const BlendSour
 
   for (int base = 0; base < n; base += kBatch) {
     if (__syncthreads_and(done0 && done1)) break;
-    stage_batch(src, range.x, base, min(kBatch, n - base), /*reverse=*/false, s_a, s_b, kColor ? s_c : nullptr,
-                nullptr);
+    stage_batch<kColor>(src, range.x, base, min(kBatch, n - base), /*reverse=*/false, s_a, s_b, s_c, nullptr);
     __syncthreads();
     const int cnt = min(kBatch, n - base);
     bool warp_done = __all_sync(kFullMask, done0 && done1);

@@ -322,6 +322,9 @@ int render_impl(const OmnigsLonlatForwardArgs* a, void* geom, size_t geom_bytes,
   d.tkeys = tkeys[0];
   d.tvals = tvals[0];
   d.scan_state = at<unsigned long long>(geom, GL.dup_scan);
+  d.incl = dkeys[0];  // free once the last depth pass has read it (the sorted keys are in dkeys[1])
+  d.emit_first = at<uint32_t>(binning, BL.emit_first);
+  d.emit_last = at<uint32_t>(binning, BL.emit_last);
   d.capacity = capacity;
   d.hdr = hdr;
   d.hist = hist + kDepthPasses * kRadix;
@@ -436,7 +439,7 @@ int omnigs_debug_lookback_timeout(const OmnigsLonlatForwardArgs* a, void* geom, 
   g_last_error.clear();
   if (a == nullptr || status == nullptr) return fail(OMNIGS_ERR_INVALID_ARGUMENT, "NULL argument");
   if (max_spins <= 0) return fail(OMNIGS_ERR_INVALID_ARGUMENT, "max_spins must be positive");
-  if (a->P <= kScanBlock)
+  if (a->P <= kScanTile)
     return fail(OMNIGS_ERR_INVALID_ARGUMENT, "the look-back probe needs more than one scan tile of Gaussians");
   if (int rc = omnigs_lonlat_preprocess(a, geom, geom_bytes, stream)) return rc;
   const LookbackProbe probe{max_spins};

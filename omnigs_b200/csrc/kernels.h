@@ -86,6 +86,10 @@ struct DuplicateParams {
   uint32_t* tkeys;             // [capacity] tile ids
   uint32_t* tvals;             // [capacity] record indices
   unsigned long long* scan_state;
+  uint32_t* incl;              // [V][P] scratch: inclusive instance offsets in depth order
+                               // (the depth sort's first key buffer, free after its last pass)
+  uint32_t* emit_first;        // [emit_blocks(capacity) + 1]: depth-order position of the Gaussian
+  uint32_t* emit_last;         // holding each emit block's first / last instance
   int64_t capacity;
   GeomHeader* hdr;
   int seam_wrap;               // tile columns wrap modulo gx (rects from tile_rect_cyclic)

@@ -15,7 +15,8 @@
 //                                tile ranges uint2[tiles]  (tile ranges only with
 //                                OMNIGS_FLAG_RECOMPUTE_T: the backward recomputes the rest)
 //   binning (per instance, capacity C): tile keys u32[2][C] | Gaussian indices u32[2][C] |
-//                                digit histograms u32[7][256] | tile-sort look-back u32[3][tiles][256]
+//                                digit histograms u32[7][256] | tile-sort look-back u32[3][tiles][256] |
+//                                duplicate emit-block index u32[2][C / 2048 + 1]
 //
 // Every array starts on a 256-byte boundary.
 #pragma once
@@ -33,13 +34,16 @@ namespace omnigs {
 
 constexpr size_t kAlign = 256;
 constexpr int kMaxBatchViews = 32;           // views per batched launch
-constexpr int kScanBlock = 256;          // Gaussians per preprocess / duplicate block
+constexpr int kScanBlock = 256;          // threads of a preprocess / duplicate block
 constexpr int kSortThreads = 256;
 constexpr int kSortItems = 16;           // keys per thread per sort tile
 constexpr int kSortTile = kSortThreads * kSortItems;
 constexpr int kRadixBits = 8;
 constexpr int kRadix = 1 << kRadixBits;
 constexpr int kDepthPasses = 4;          // 32-bit depth keys, 8-bit digits
+// The depth sort ping-pongs between two key buffers; with an even pass count its result lands in
+// the second, and the duplicate pass uses the first as scratch.
+static_assert(kDepthPasses % 2 == 0, "the duplicate pass's scratch is the depth sort's first key buffer");
 constexpr int kTilePasses = 3;           // tile ids (<= 21 bits): up to three digits of <= 8 bits
 constexpr int kMaxSortPasses = kDepthPasses + kTilePasses;
 constexpr int64_t kMaxInstances = (int64_t(1) << 30) - 1;  // look-back words hold 30-bit counts
@@ -109,8 +113,16 @@ struct ImageLayout {
   }
 };
 
+// The duplicate pass writes the instance list in blocks of kEmitBlock instances; its scan records,
+// per such block, the depth-order positions of the Gaussians holding the block's first and last
+// instance (emit_first / emit_last).
+constexpr int kEmitBlock = 2048;
+inline int64_t emit_blocks(int64_t capacity) { return (capacity + kEmitBlock - 1) / kEmitBlock; }
+// Gaussians per block of the duplicate's scan (4 per thread)
+constexpr int kScanTile = 1024;
+
 struct BinningLayout {
-  size_t tkeys0, tkeys1, tvals0, tvals1, hist, tile_lookback, total;
+  size_t tkeys0, tkeys1, tvals0, tvals1, hist, tile_lookback, emit_first, emit_last, total;
   int64_t capacity;
   static BinningLayout make(int64_t C) {
     BinningLayout L;
@@ -123,6 +135,8 @@ struct BinningLayout {
     L.hist = o; o = align_up(o + sizeof(uint32_t) * kMaxSortPasses * kRadix);
     // room for a per-view tile sort of a batch: up to kMaxBatchViews more (partial) tiles per pass
     L.tile_lookback = o; o = align_up(o + sizeof(uint32_t) * kTilePasses * (sort_tiles(C) + kMaxBatchViews) * kRadix);
+    L.emit_first = o; o = align_up(o + sizeof(uint32_t) * (emit_blocks(C) + 1));
+    L.emit_last = o; o = align_up(o + sizeof(uint32_t) * (emit_blocks(C) + 1));
     L.total = o;
     return L;
   }

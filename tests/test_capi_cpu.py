@@ -271,13 +271,13 @@ def test_blend_batch_setting():
 
 @pytest.mark.parametrize("sizes,P,passes", [
     ([(3072, 1536)] * 4 + [(512, 256)], 20_000, 2),   # 74,240 tiles (17 bits) vs 18,432 per view (15)
-    ([(3072, 1536)] * 4 + [(512, 256)], 200, 3),      # P < 256: the global tile sort
+    ([(3072, 1536)] * 4 + [(512, 256)], 200, 2),      # small P: per view as well
     ([(3072, 1536)], 20_000, 2),                      # one view: its own 15-bit ids
     ([(2048, 1024), (512, 256), (3072, 1536)], 20_000, 2),  # 27,136 tiles: two passes either way
 ])
 def test_batch_tile_sort_runs_per_view_when_it_saves_a_pass(sizes, P, passes):
     """The batched tile sort works on view-local tile ids when that needs fewer digit passes than
-    the batch's global ids (and P >= 256); state_view reports the passes of the sort that runs."""
+    the batch's global ids; state_view reports the passes of the sort that runs."""
     V = len(sizes)
     W = (ctypes.c_int * V)(*[w for w, _ in sizes])
     H = (ctypes.c_int * V)(*[h for _, h in sizes])
