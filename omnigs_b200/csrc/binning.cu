@@ -34,6 +34,9 @@ constexpr uint32_t kLbValue = (1u << 30) - 1;
 constexpr unsigned long long kScanAggregate = 1ull << 62;
 constexpr unsigned long long kScanPrefix = 2ull << 62;
 constexpr unsigned long long kScanValue = (1ull << 62) - 1;
+// Predecessors a look-back reads per round.  Measured on a B200 (1M Gaussians, 2048x1024): 16 or
+// 32 per round made every sort pass slower (depth passes 21 -> 24-27 us, tile passes 90 -> 95-125
+// us), so the walk is not bound by its round trips.
 constexpr int kLookbackBatch = 8;
 
 __device__ __forceinline__ bool instances_fit(const GeomHeader* hdr, int64_t capacity) {
@@ -348,9 +351,10 @@ __global__ void __launch_bounds__(kSortThreads, 3) onesweep_kernel(OnesweepParam
 //  2. instance_emit_kernel: block b writes instances [2048 b, 2048 b + 2048) of the list: every
 //     block does the same amount of work however the instances are spread over the Gaussians
 //     (the nearest splats, first in depth order, cover thousands of tiles each).  It stages the
-//     offsets and tile rects of its Gaussians in shared memory, each thread finds its instances'
-//     Gaussians by binary search there, and counts the digit histograms of the tile sort that
-//     follows while writing the keys.
+//     offsets and tile rects of its Gaussians in shared memory; each thread writes 8 consecutive
+//     instances (one binary search for the first one's Gaussian, then a walk through the rect and
+//     on to the next Gaussians, two 16-byte stores per array) and counts the digit histograms of
+//     the tile sort that follows.
 // One kernel doing both measured ~150 us at 400k and 1M Gaussians alike: a block's warps each
 // emitted their own Gaussians' instances, so a block held its SM slots until its busiest warp was
 // done (62 % of the stall samples were barrier waits).
@@ -416,7 +420,13 @@ __global__ void __launch_bounds__(kScanBlock) instance_scan_kernel(const __grid_
 #pragma unroll
   for (int u = 0; u < kScanItems; ++u) {
     const uint32_t i = i0 + u;
-    cnt[u] = i < items ? record_rect<kPerView>(p, p.order[i], record_view(p, i)).count : 0u;
+    cnt[u] = 0;
+    if (i < items) {
+      const RecordRect r = record_rect<kPerView>(p, p.order[i], record_view(p, i));
+      cnt[u] = r.count;
+      p.rect_row[i] = r.row_origin;
+      p.rect_cw[i] = ((uint32_t)r.col0 & 0xffffu) | ((uint32_t)r.width << 16);
+    }
   }
   uint32_t thread_total = 0;
 #pragma unroll
@@ -514,7 +524,7 @@ __global__ void __launch_bounds__(kScanBlock) instance_scan_kernel(const __grid_
 }
 
 constexpr int kEmitPerThread = kEmitBlock / kScanBlock;
-constexpr int kEmitStage = kEmitBlock + 1;  // Gaussians of a block staged in shared memory
+constexpr int kEmitStage = 1025;  // Gaussians of a block staged in shared memory (more: read from global memory)
 
 __device__ __forceinline__ float rcp_approx_f(float x) {
   float r;
@@ -553,75 +563,99 @@ __global__ void __launch_bounds__(kScanBlock) instance_emit_kernel(const __grid_
     for (uint32_t t = threadIdx.x; t < n; t += kScanBlock) {
       const uint32_t i = g_first + t;
       const uint32_t view = record_view(p, i);
-      const uint32_t rec = p.order[i];
-      const RecordRect r = record_rect<kPerView>(p, rec, view);
       s_incl[t] = p.incl[i];
-      s_rec[t] = rec;
-      s_row[t] = r.row_origin;
-      s_cw[t] = ((uint32_t)r.col0 & 0xffffu) | ((uint32_t)r.width << 16);
-      s_pv[t] = (uint32_t)r.pitch | (view << 16);
+      s_rec[t] = p.order[i];
+      s_row[t] = p.rect_row[i];
+      s_cw[t] = p.rect_cw[i];
+      s_pv[t] = (uint32_t)p.gx[view] | (view << 16);
     }
   __syncthreads();
   const uint32_t* incl = staged ? s_incl : p.incl + g_first;
   const uint32_t excl0 = g_first > 0 ? p.incl[g_first - 1] : 0u;
   const uint32_t view0 = record_view(p, g_first);
-#pragma unroll 2
-  for (int k = 0; k < kEmitPerThread; ++k) {
-    const uint32_t o = o_lo + (uint32_t)(k * kScanBlock) + threadIdx.x;
-    const bool ok = o < o_hi;
-    uint32_t key = 0, view = view0;
-    if (ok) {
-      // j: the first of the block's Gaussians whose inclusive offset exceeds o
-      uint32_t lo = 0, hi = n - 1u;
-      while (lo < hi) {
-        const uint32_t mid = (lo + hi) >> 1;
-        if (incl[mid] > o)
-          hi = mid;
-        else
-          lo = mid + 1u;
-      }
-      const uint32_t start = lo > 0 ? incl[lo - 1] : excl0;
-      uint32_t rec, row_origin;
-      int col0, width, pitch;
-      if (staged) {
-        rec = s_rec[lo];
-        row_origin = s_row[lo];
-        const uint32_t cw = s_cw[lo], pv = s_pv[lo];
-        col0 = (int)(int16_t)(cw & 0xffffu);
-        width = (int)(cw >> 16);
-        pitch = (int)(pv & 0xffffu);
-        view = pv >> 16;
-      } else {
-        view = record_view(p, g_first + lo);
-        rec = p.order[g_first + lo];
-        const RecordRect r = record_rect<kPerView>(p, rec, view);
-        row_origin = r.row_origin;
-        col0 = r.col0;
-        width = r.width;
-        pitch = r.pitch;
-      }
-      const uint32_t local = o - start;
-      // local / width from an approximate reciprocal: local < 2^21 (a rect holds at most every
-      // tile of a view), so the truncated estimate is within one of the quotient; one step fixes it
-      uint32_t ry = (uint32_t)((float)local * rcp_approx_f((float)width));
-      int rem = (int)(local - ry * (uint32_t)width);
-      if (rem < 0) {
-        ry -= 1u;
-        rem += width;
-      } else if (rem >= width) {
-        ry += 1u;
-        rem -= width;
-      }
-      int tx = col0 + rem;
-      if (tx < 0) tx += pitch;  // seam wrap: columns left of 0 or right of gx - 1
-      if (tx >= pitch) tx -= pitch;
-      key = row_origin + ry * (uint32_t)pitch + (uint32_t)tx;
-      p.tkeys[o] = key;
-      p.tvals[o] = rec;
+  // Thread t writes the kEmitPerThread consecutive instances from o0: one binary search finds the
+  // Gaussian of the first, the others step through the rect (or on to the next Gaussians with
+  // instances, whose first instance they then are) without a search or a division.
+  const uint32_t o0 = o_lo + (uint32_t)threadIdx.x * (uint32_t)kEmitPerThread;
+  uint32_t j = 0;  // the first of the block's Gaussians whose inclusive offset exceeds o0
+  {
+    uint32_t hi = n - 1u;
+    while (j < hi) {
+      const uint32_t mid = (j + hi) >> 1;
+      if (incl[mid] > o0)
+        hi = mid;
+      else
+        j = mid + 1u;
     }
+  }
+  uint32_t end_j = incl[j];
+  uint32_t rec = 0, row_origin = 0, view = view0;
+  int col0 = 0, width = 1, pitch = 1;
+  auto load_rect = [&](uint32_t jj) {
+    uint32_t cw;
+    if (staged) {
+      rec = s_rec[jj];
+      row_origin = s_row[jj];
+      cw = s_cw[jj];
+      const uint32_t pv = s_pv[jj];
+      pitch = (int)(pv & 0xffffu);
+      view = pv >> 16;
+    } else {
+      const uint32_t i = g_first + jj;
+      view = record_view(p, i);
+      rec = p.order[i];
+      row_origin = p.rect_row[i];
+      cw = p.rect_cw[i];
+      pitch = p.gx[view];
+    }
+    col0 = (int)(int16_t)(cw & 0xffffu);
+    width = (int)(cw >> 16);
+  };
+  load_rect(j);
+  // row and column of o0 in the rect: local / width from an approximate reciprocal (local < 2^21,
+  // a rect holds at most every tile of a view, so the truncated estimate is within one of the
+  // quotient; one step fixes it)
+  const uint32_t local = o0 - (j > 0 ? incl[j - 1] : excl0);
+  uint32_t ry = (uint32_t)((float)local * rcp_approx_f((float)width));
+  int rem = (int)(local - ry * (uint32_t)width);
+  if (rem < 0) {
+    ry -= 1u;
+    rem += width;
+  } else if (rem >= width) {
+    ry += 1u;
+    rem -= width;
+  }
+  uint32_t keys[kEmitPerThread], vals[kEmitPerThread];
+  const uint32_t slot_limit = kPerView ? (uint32_t)kSlots : 1u;
+#pragma unroll
+  for (int k = 0; k < kEmitPerThread; ++k) {
+    const uint32_t o = o0 + (uint32_t)k;
+    const bool ok = o < o_hi;
+    if (k > 0 && ok) {
+      // past Gaussian j: on to the next one that has instances, whose first instance o is (j stays
+      // below n even after an inconsistent scan, which the status word reports)
+      if (o >= end_j && j + 1u < n) {
+        do {
+          ++j;
+          end_j = incl[j];
+        } while (end_j <= o && j + 1u < n);
+        load_rect(j);
+        ry = 0;
+        rem = 0;
+      } else if (++rem == width) {
+        rem = 0;
+        ++ry;
+      }
+    }
+    int tx = col0 + rem;
+    if (tx < 0) tx += pitch;  // seam wrap: columns left of 0 or right of gx - 1
+    if (tx >= pitch) tx -= pitch;
+    const uint32_t key = row_origin + ry * (uint32_t)pitch + (uint32_t)tx;
+    keys[k] = key;
+    vals[k] = rec;
     // digit histograms of the tile sort (the pass that would otherwise re-read every key)
     const uint32_t slot = kPerView ? view - view0 : 0u;
-    const bool counted = ok && slot < (uint32_t)kSlots;
+    const bool counted = ok && slot < slot_limit;
     const unsigned live = __ballot_sync(kFullMask, counted);
 #pragma unroll
     for (int q = 0; q < kTilePasses; ++q)
@@ -630,6 +664,24 @@ __global__ void __launch_bounds__(kScanBlock) instance_emit_kernel(const __grid_
         count_digit(s_hist, slot * kHistSlot + q * kRadix + digit, counted, live, lane);
         if (kPerView && ok && !counted)
           atomicAdd(&p.hist[(size_t)view * kHistSlot + q * kRadix + digit], 1u);
+      }
+  }
+  // the thread's run of the list: 16-byte stores when it is whole (o0 is a multiple of 8, the
+  // lists start 256-byte aligned)
+  static_assert(kEmitPerThread == 8, "two 16-byte stores per array");
+  if (o0 + (uint32_t)kEmitPerThread <= o_hi) {
+    uint4* kd = reinterpret_cast<uint4*>(p.tkeys + o0);
+    uint4* vd = reinterpret_cast<uint4*>(p.tvals + o0);
+    kd[0] = make_uint4(keys[0], keys[1], keys[2], keys[3]);
+    kd[1] = make_uint4(keys[4], keys[5], keys[6], keys[7]);
+    vd[0] = make_uint4(vals[0], vals[1], vals[2], vals[3]);
+    vd[1] = make_uint4(vals[4], vals[5], vals[6], vals[7]);
+  } else {
+#pragma unroll
+    for (int k = 0; k < kEmitPerThread; ++k)
+      if (o0 + (uint32_t)k < o_hi) {
+        p.tkeys[o0 + k] = keys[k];
+        p.tvals[o0 + k] = vals[k];
       }
   }
   if (p.hist_passes == 0) return;

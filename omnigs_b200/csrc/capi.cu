@@ -323,6 +323,10 @@ int render_impl(const OmnigsLonlatForwardArgs* a, void* geom, size_t geom_bytes,
   d.tvals = tvals[0];
   d.scan_state = at<unsigned long long>(geom, GL.dup_scan);
   d.incl = dkeys[0];  // free once the last depth pass has read it (the sorted keys are in dkeys[1])
+  // the depth sort's other free buffers: its sorted keys and its first value buffer
+  static_assert(((kDepthPasses - 1) & 1) == 1, "the depth order is in dvals[1]");
+  d.rect_row = dvals[0];
+  d.rect_cw = dkeys[1];
   d.emit_first = at<uint32_t>(binning, BL.emit_first);
   d.emit_last = at<uint32_t>(binning, BL.emit_last);
   d.capacity = capacity;

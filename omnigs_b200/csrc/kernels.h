@@ -88,6 +88,10 @@ struct DuplicateParams {
   unsigned long long* scan_state;
   uint32_t* incl;              // [V][P] scratch: inclusive instance offsets in depth order
                                // (the depth sort's first key buffer, free after its last pass)
+  // [V][P] scratch in depth order, written by the scan for the emission: each Gaussian's first
+  // row's tile id and its first column | width << 16 (the depth sort's free buffers)
+  uint32_t* rect_row;
+  uint32_t* rect_cw;
   uint32_t* emit_first;        // [emit_blocks(capacity) + 1]: depth-order position of the Gaussian
   uint32_t* emit_last;         // holding each emit block's first / last instance
   int64_t capacity;
