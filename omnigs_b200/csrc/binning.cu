@@ -36,7 +36,10 @@ constexpr unsigned long long kScanPrefix = 2ull << 62;
 constexpr unsigned long long kScanValue = (1ull << 62) - 1;
 // Predecessors a look-back reads per round.  Measured on a B200 (1M Gaussians, 2048x1024): 16 or
 // 32 per round made every sort pass slower (depth passes 21 -> 24-27 us, tile passes 90 -> 95-125
-// us), so the walk is not bound by its round trips.
+// us), so the walk is not bound by its round trips.  Nor is the pass bound by its look-back: a
+// reduce-then-scan in its place (a kernel counting every tile's digits and scanning the counts
+// over the tiles, then the pass without waits) made the sort slower, 0.294 -> 0.366 ms per view:
+// the count kernels took 12-27 us each and the passes got only 4-10 us faster.
 constexpr int kLookbackBatch = 8;
 
 __device__ __forceinline__ bool instances_fit(const GeomHeader* hdr, int64_t capacity) {
@@ -148,7 +151,7 @@ __device__ __forceinline__ uint32_t block_exclusive_scan(uint32_t v, uint32_t* s
 }
 
 // One stable LSD pass over (u32 key, u32 value) pairs on the digit (key >> shift) & mask.  A block
-// ranks a 4096-item tile in shared memory (warp multi-split with match.any: equal digits keep
+// ranks a 4096-item tile in shared memory (warp multi-split from per-bit ballots: equal digits keep
 // their input order), publishes its per-digit counts, resolves its global digit offsets by
 // decoupled look-back (tiles are taken in launch order from an atomic counter, so a block only
 // waits on blocks that are already running) and writes runs of equal digits coalesced.  In a
@@ -247,14 +250,21 @@ __global__ void __launch_bounds__(kSortThreads, 3) onesweep_kernel(OnesweepParam
   for (int k = 0; k < kItems; ++k) {
     const bool valid = tile_base + k * 32 < n;
     const uint32_t digit = (key[k] >> shift) & mask;
-    const unsigned peers = __match_any_sync(kFullMask, valid ? digit : (0x10000u | lane));
-    const int leader = __ffs(peers) - 1;
-    uint32_t old = 0;
-    if (valid && lane == leader) {
-      old = sm.warp_hist[warp][digit];
-      sm.warp_hist[warp][digit] = old + __popc(peers);
+    // the valid lanes holding the same digit: one ballot per digit bit (measured faster on a B200
+    // than match.any: depth passes 21 -> 18 us, tile passes 86-96 -> 80 us at 1M Gaussians)
+    unsigned peers = __ballot_sync(kFullMask, valid);
+#pragma unroll
+    for (int b = 0; b < kRadixBits; ++b) {
+      const bool bit = (digit >> b) & 1u;
+      const unsigned bal = __ballot_sync(kFullMask, bit);
+      peers &= bit ? bal : ~bal;
     }
-    old = __shfl_sync(kFullMask, old, leader);
+    if (!valid) peers = 1u << lane;
+    const int leader = __ffs(peers) - 1;
+    // every lane reads its digit's running count; the digit's first lane then advances it
+    const uint32_t old = valid ? sm.warp_hist[warp][digit] : 0u;
+    __syncwarp();
+    if (valid && lane == leader) sm.warp_hist[warp][digit] = old + __popc(peers);
     __syncwarp();
     rank[k] = valid ? (old + __popc(peers & lt_mask)) : 0xffffffffu;
   }
