@@ -15,7 +15,9 @@
  * Optional inputs are NULL, as the reference's empty tensors are.
  *
  * The three state buffers (geometry, binning, image) are caller-owned device memory whose sizes
- * come from the *_bytes queries; their layout is private to this library.  Nothing here allocates
+ * come from the *_bytes queries; their layout is private to this library.  They (and the batch
+ * state buffer) must start on a 16-byte boundary, as cudaMalloc and the PyTorch allocator give
+ * (OMNIGS_ERR_INVALID_ARGUMENT otherwise).  Nothing here allocates
  * device memory and nothing synchronises the host except omnigs_lonlat_read_status and
  * omnigs_lonlat_forward_early_status.  The instance count (num_rendered) is produced and consumed
  * on the device; the binning buffer is sized for a caller-chosen capacity and a pass that would

@@ -180,7 +180,7 @@ BatchRenderParams render_params(const BatchParams& p, const BatchPlan& plan, voi
 int check_state(const BatchLayout& L, void* state, size_t state_bytes) {
   if (state == nullptr || state_bytes < L.total)
     return fail(OMNIGS_ERR_BUFFER_TOO_SMALL, "batch state smaller than omnigs_batch_state_bytes()");
-  return OMNIGS_OK;
+  return check_aligned(state);
 }
 
 }  // namespace
@@ -216,6 +216,7 @@ int omnigs_batch_render(const OmnigsBatchArgs* a, void* state, size_t state_byte
   int64_t capacity = BinningLayout::capacity_for(binning_bytes);
   if (binning == nullptr || capacity < 0)
     return fail(OMNIGS_ERR_BUFFER_TOO_SMALL, "binning buffer smaller than omnigs_lonlat_binning_bytes(0)");
+  if (int rc = check_aligned(binning)) return rc;
   const BinningLayout BL = BinningLayout::make(capacity);
   if (capacity > kMaxInstances) capacity = kMaxInstances;
   const BatchParams bp = batch_params(a, plan, state, L);
@@ -365,6 +366,7 @@ int omnigs_batch_forward(const OmnigsBatchArgs* a, void* state, size_t state_byt
   if (a->P > 0) {
     const BatchLayout L = batch_layout(a->P, plan);
     if (int rc = check_state(L, state, state_bytes)) return rc;
+    if (int rc = check_aligned(binning)) return rc;  // before the preprocess's device work
     cudaStream_t s = reinterpret_cast<cudaStream_t>(stream);
     if (cudaMemsetAsync(state, 0, L.dup_scan, s) != cudaSuccess) return check_launch("memset batch header");
     const BatchParams bp = batch_params(a, plan, state, L);
@@ -392,6 +394,7 @@ int omnigs_batch_backward(const OmnigsBatchArgs* a, const OmnigsBatchGrads* g, v
   int64_t capacity = BinningLayout::capacity_for(binning_bytes);
   if (binning == nullptr || capacity < 0)
     return fail(OMNIGS_ERR_BUFFER_TOO_SMALL, "binning buffer smaller than omnigs_lonlat_binning_bytes(0)");
+  if (int rc = check_aligned(binning)) return rc;
   const BinningLayout BL = BinningLayout::make(capacity);
   if (capacity > kMaxInstances) capacity = kMaxInstances;
   const int fin = batch_tile_sort(plan).digits.passes & 1;
@@ -437,6 +440,7 @@ int omnigs_batch_autotune(const OmnigsBatchArgs* a, void* state, size_t state_by
   int64_t capacity = BinningLayout::capacity_for(binning_bytes);
   if (binning == nullptr || capacity < 0)
     return fail(OMNIGS_ERR_BUFFER_TOO_SMALL, "binning buffer smaller than omnigs_lonlat_binning_bytes(0)");
+  if (int rc = check_aligned(binning)) return rc;
   const BinningLayout BL = BinningLayout::make(capacity);
   if (capacity > kMaxInstances) capacity = kMaxInstances;
   cudaStream_t s = reinterpret_cast<cudaStream_t>(stream);

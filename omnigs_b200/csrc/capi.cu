@@ -58,6 +58,13 @@ __global__ void begin_render_kernel(GeomHeader* hdr) {
 
 void launch_begin_render(GeomHeader* hdr, cudaStream_t s) { begin_render_kernel<<<1, 1, 0, s>>>(hdr); }
 
+int check_aligned(const void* a, const void* b, const void* c) {
+  for (const void* q : {a, b, c})
+    if ((reinterpret_cast<uintptr_t>(q) & 15) != 0)
+      return fail(OMNIGS_ERR_INVALID_ARGUMENT, "workspace buffers must be 16-byte aligned");
+  return OMNIGS_OK;
+}
+
 int validate_common(int P, int D, int M, int W, int H, const void* shs, const float* colors,
                     const float* scales, const float* rotations, const float* cov3D,
                     const float* means3D, const float* viewmatrix, const float* campos) {
@@ -166,6 +173,7 @@ int omnigs_lonlat_preprocess(const OmnigsLonlatForwardArgs* a, void* geom, size_
   const GeomLayout L = GeomLayout::make(a->P);
   if (geom == nullptr || geom_bytes < L.total)
     return fail(OMNIGS_ERR_BUFFER_TOO_SMALL, "geometry buffer smaller than omnigs_lonlat_geom_bytes(P)");
+  if (int rc = check_aligned(geom)) return rc;
   if (cudaMemsetAsync(geom, 0, sizeof(GeomHeader), s) != cudaSuccess) return check_launch("memset geometry header");
   if (a->P == 0) return OMNIGS_OK;
   PreprocessParams p{};
@@ -258,6 +266,7 @@ int render_impl(const OmnigsLonlatForwardArgs* a, void* geom, size_t geom_bytes,
   int64_t capacity = BinningLayout::capacity_for(binning_bytes);
   if (binning == nullptr || capacity < 0)
     return fail(OMNIGS_ERR_BUFFER_TOO_SMALL, "binning buffer smaller than omnigs_lonlat_binning_bytes(0)");
+  if (int rc = check_aligned(geom, image, binning)) return rc;
   const BinningLayout BL = BinningLayout::make(capacity);
   if (capacity > kMaxInstances) capacity = kMaxInstances;
   const int gx = tiles_x(a->W), gy = tiles_y(a->H);
@@ -411,6 +420,7 @@ int omnigs_lonlat_render(const OmnigsLonlatForwardArgs* a, void* geom, size_t ge
 int omnigs_lonlat_forward(const OmnigsLonlatForwardArgs* a, void* geom, size_t geom_bytes,
                           void* binning, size_t binning_bytes, void* image, size_t image_bytes,
                           omnigs_stream_t stream) {
+  if (int rc = check_aligned(geom, binning, image)) return rc;  // before the preprocess's device work
   if (int rc = omnigs_lonlat_preprocess(a, geom, geom_bytes, stream)) return rc;
   return omnigs_lonlat_render(a, geom, geom_bytes, binning, binning_bytes, image, image_bytes, stream);
 }
@@ -420,6 +430,7 @@ int omnigs_lonlat_forward_early_status(const OmnigsLonlatForwardArgs* a, void* g
                                        int* num_rendered, uint32_t* status, omnigs_stream_t stream) {
   if (num_rendered == nullptr || status == nullptr)
     return fail(OMNIGS_ERR_INVALID_ARGUMENT, "num_rendered and status must not be NULL");
+  if (int rc = check_aligned(geom, binning, image)) return rc;  // before the preprocess's device work
   if (int rc = omnigs_lonlat_preprocess(a, geom, geom_bytes, stream)) return rc;
   g_last_error.clear();
   if (a->P == 0) {
@@ -498,6 +509,7 @@ int omnigs_lonlat_backward(const OmnigsLonlatBackwardArgs* a, void* geom, size_t
   const int64_t capacity = BinningLayout::capacity_for(binning_bytes);
   if (binning == nullptr || capacity < 0)
     return fail(OMNIGS_ERR_BUFFER_TOO_SMALL, "binning buffer smaller than omnigs_lonlat_binning_bytes(0)");
+  if (int rc = check_aligned(geom, image, binning)) return rc;
   if (a->R > capacity) return fail(OMNIGS_ERR_CAPACITY, "R exceeds the binning buffer's capacity");
   const BinningLayout BL = BinningLayout::make(capacity);
   const int gx = tiles_x(a->W), gy = tiles_y(a->H);
@@ -533,6 +545,7 @@ int omnigs_lonlat_backward(const OmnigsLonlatBackwardArgs* a, void* geom, size_t
   b.radii = a->radii;
   b.shs = a->shs;
   b.color = at<float4>(geom, GL.color);
+  b.splat = at<float4>(geom, GL.splat);
   b.scales = a->scales;
   b.rotations = a->rotations;
   b.cov3D_precomp = a->cov3D_precomp;

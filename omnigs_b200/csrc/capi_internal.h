@@ -27,6 +27,10 @@ int validate_common(int P, int D, int M, int W, int H, const void* shs, const fl
                     const float* scales, const float* rotations, const float* cov3D,
                     const float* means3D, const float* viewmatrix, const float* campos);
 
+// OMNIGS_ERR_INVALID_ARGUMENT unless every given workspace buffer (NULL: not given) is 16-byte
+// aligned: the kernels move their records with 16-byte loads and stores.
+int check_aligned(const void* a, const void* b = nullptr, const void* c = nullptr);
+
 template <class T>
 T* at(void* base, size_t off) {
   return reinterpret_cast<T*>(static_cast<unsigned char*>(base) + off);

@@ -146,6 +146,7 @@ struct PreprocessBackwardParams {
   const int* radii;
   const float* shs;
   const float4* color;  // clamp bits in .w
+  const float4* splat;  // [P][2] splat records (their conic turns the blend's mean sums into terms)
   const float* scales;
   const float* rotations;
   const float* cov3D_precomp;

@@ -44,12 +44,17 @@ __global__ void __launch_bounds__(256) preprocess_backward_kernel(PreprocessBack
   const float4 g0 = p.grad_acc[3 * idx];
   const float4 g1 = p.grad_acc[3 * idx + 1];
   const float4 g2 = p.grad_acc[3 * idx + 2];
+  // the blend sums q dx and q dy (turned into the mean terms by the conic here) and the conic
+  // terms, all without their constant factors (render_bwd.cu); the conic is read before the record
+  // is cleared (the compiler cannot move loads of possibly aliasing memory past those stores)
+  const float4 sa = __ldg(&p.splat[2 * idx]);  // {x, y, conic a, conic b}
+  const float conic_c = __ldg(&p.splat[2 * idx + 1].x);
   const float4 z4 = make_float4(0.f, 0.f, 0.f, 0.f);
   p.grad_acc[3 * idx] = z4;
   p.grad_acc[3 * idx + 1] = z4;
   p.grad_acc[3 * idx + 2] = z4;
-  // the blend sums the mean and conic terms without their constant factors (render_bwd.cu)
-  const float dmean2D_x = -0.5f * (float)p.W * g0.x, dmean2D_y = -0.5f * (float)p.H * g0.y;
+  const float mx = fmaf(sa.z, g0.x, sa.w * g0.y), my = fmaf(sa.w, g0.x, conic_c * g0.y);
+  const float dmean2D_x = -0.5f * (float)p.W * mx, dmean2D_y = -0.5f * (float)p.H * my;
   const float3 dL_dconic = {-0.5f * g0.z, -0.5f * g0.w, -0.5f * g1.x};
   const float dL_dcolor[3] = {g1.z, g1.w, g2.x};
   p.dL_dmeans2D[3 * idx] = dmean2D_x;

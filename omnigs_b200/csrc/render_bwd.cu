@@ -9,8 +9,9 @@
 // 1 - alpha serves both of the reference's divisions by it (relative error ~1e-7 per step, far
 // inside the gradients' 1e-3 tolerance).  The per-(pixel, splat) gradients (2 screen-space mean,
 // 3 conic, 1 opacity, 3 colour) are not pushed with 9 global atomics per pixel as in the
-// reference (and the mean and conic terms are summed without their constant factors -W/2, -H/2,
-// -1/2, which the backward preprocess applies per Gaussian): a thread first sums them over its two
+// reference (and the mean terms are summed as q dx and q dy without the conic, the mean and conic
+// terms without their constant factors -W/2, -H/2, -1/2: the backward preprocess applies those
+// per Gaussian): a thread first sums them over its two
 // pixels and writes the 9 sums to its warp's shared buffer; every second contributing splat the
 // warp that owns the 8 x 8 patch reduces the buffer transposed (one lane per splat and value, 32
 // terms each) and adds the accumulator records with one atomic per value.  Warps skip splats
@@ -177,17 +178,17 @@ __device__ __forceinline__ void blend_backward_tile(const TileJob& job, const Bl
             // With q = G dL/dG = o G dL/dalpha and the conic (a, b, c):
             //   dL/d(delta x) = -q (a dx + b dy), dL/d(delta y) = -q (c dy + b dx),
             //   dL/d(conic) = -q (dx^2, dx dy, dy^2) / 2.
-            // The per-pixel sums keep only q (a dx + b dy), ...; the constant factors -W/2, -H/2 and
-            // -1/2 are applied once per Gaussian by the backward preprocess.
-            // The thread's two pixels share dx, so the sums over them factor through
-            // sum q, sum q dy and sum q dy^2.
+            // The per-pixel sums keep only q dx, q dy, q dx^2, ...: the conic (constant over the
+            // Gaussian's pixels) and the constant factors -W/2, -H/2 and -1/2 are applied once per
+            // Gaussian by the backward preprocess.  The thread's two pixels share dx, so the sums
+            // over them factor through sum q, sum q dy and sum q dy^2.
             const float2 w5 = mul2(Ge, dLda);
             const float2 q = mul2(f2(b.y), w5);
             const float2 qy = mul2(q, dy);
             const float qs = q.x + q.y, qdy = qy.x + qy.y;
-            v[0] = fmaf(a.z * dx, qs, a.w * qdy);
-            v[1] = fmaf(a.w * dx, qs, b.x * qdy);
-            v[2] = dx * dx * qs;
+            v[0] = dx * qs;
+            v[1] = qdy;
+            v[2] = dx * v[0];
             v[3] = dx * qdy;
             v[4] = fmaf(qy.x, dy.x, qy.y * dy.y);
             v[5] = w5.x + w5.y;

@@ -93,6 +93,29 @@ def test_forward_rejects_small_buffers():
     assert b"geometry" in capi.lib().omnigs_last_error()
 
 
+def test_misaligned_workspace_buffers_are_rejected_before_device_work():
+    # the kernels move their records with 16-byte accesses; cudaMalloc and torch align to 256 B
+    L = capi.lib()
+    a = _fake_args()
+    off = 0x10008
+    assert L.omnigs_lonlat_preprocess(ctypes.byref(a), off, 1 << 30, None) == 1
+    assert b"16-byte" in L.omnigs_last_error()
+    for geom, binning, image in ((off, 0x10000, 0x10000), (0x10000, off, 0x10000), (0x10000, 0x10000, off)):
+        rc = L.omnigs_lonlat_forward(ctypes.byref(a), geom, 1 << 30, binning, 1 << 30, image, 1 << 30, None)
+        assert rc == 1 and b"16-byte" in L.omnigs_last_error()
+    b = capi.BackwardArgs()
+    b.P, b.D, b.M, b.W, b.H, b.R = 10, 3, 16, 64, 32, 10
+    for f, _ in capi.BackwardArgs._fields_:
+        if f not in ("P", "D", "M", "W", "H", "R", "scale_modifier", "colors_precomp",
+                     "cov3D_precomp", "dL_dconic", "flags"):
+            setattr(b, f, 0x10000)
+    rc = L.omnigs_lonlat_backward(ctypes.byref(b), 0x10000, 1 << 30, off, 1 << 30, 0x10000, 1 << 30, None)
+    assert rc == 1 and b"16-byte" in L.omnigs_last_error()
+    ba, keep = _fake_batch()
+    assert L.omnigs_batch_forward(ctypes.byref(ba), off, 1 << 40, 0x10000, 1 << 40, None) == 1
+    assert L.omnigs_batch_forward(ctypes.byref(ba), 0x10000, 1 << 40, off, 1 << 40, None) == 1
+
+
 def test_backward_rejects_capacity_mismatch():
     a = capi.BackwardArgs()
     a.P, a.D, a.M, a.W, a.H, a.R = 10, 3, 16, 64, 32, 1000
