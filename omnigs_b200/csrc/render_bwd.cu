@@ -137,6 +137,8 @@ __device__ __forceinline__ void blend_backward_tile(const TileJob& job, const Bl
     for (int k = 0; k * 32 < cnt; ++k) {
       const int j = k * 32 + lane;
       bool hit = false;
+      // (the branch skips the test for splats behind every last contributor of the warp: evaluating
+      // it in every lane measured 3 % slower)
       if (j < cnt && (uint32_t)(hi - 1 - j) < warp_last) hit = patch.template hit<kWrap>(s_a[j], s_b[j]);
       unsigned m = __ballot_sync(kFullMask, hit);
       while (m) {
