@@ -172,12 +172,14 @@ __global__ void __launch_bounds__(kBatchBlock, batch_bwd_min_blocks<kFp64Poles>(
     const float4 g2 = p.grad_acc[3 * rec + 2];
     const float* vm = p.viewmatrices + 16 * v;
     const int W = p.views[v].W, H = p.views[v].H;
-    // the blend sums q dx and q dy (turned into the mean terms by the conic here) and the conic
-    // terms, all without their constant factors (render_bwd.cu)
-    const float3 dconic = {-0.5f * g0.z, -0.5f * g0.w, -0.5f * g1.x};
+    // the blend sums w dx and w dy (turned into the mean terms by the opacity and the conic here)
+    // and the conic terms (by the opacity), all without their constant factors (render_bwd.cu)
     const float4 sa = p.splat[2 * rec];  // {x, y, conic a, conic b}
-    const float conic_c = p.splat[2 * rec + 1].x;
-    const float mx = fmaf(sa.z, g0.x, sa.w * g0.y), my = fmaf(sa.w, g0.x, conic_c * g0.y);
+    const float4 sb = p.splat[2 * rec + 1];  // {conic c, opacity, ...}
+    const float conic_c = sb.x, opacity = sb.y;
+    const float mx = opacity * fmaf(sa.z, g0.x, sa.w * g0.y), my = opacity * fmaf(sa.w, g0.x, conic_c * g0.y);
+    const float ho = -0.5f * opacity;
+    const float3 dconic = {ho * g0.z, ho * g0.w, ho * g1.x};
     const float dm2x = -0.5f * (float)W * mx, dm2y = -0.5f * (float)H * my;
     float dcov_v[6];
     LonlatJacobian jac;

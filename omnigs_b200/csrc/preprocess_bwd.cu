@@ -85,19 +85,21 @@ __global__ void __launch_bounds__(kPbThreads) preprocess_backward_kernel(Preproc
     const float4 g0 = p.grad_acc[3 * idx];
     const float4 g1 = p.grad_acc[3 * idx + 1];
     const float4 g2 = p.grad_acc[3 * idx + 2];
-    // the blend sums q dx and q dy (turned into the mean terms by the conic here) and the conic
-    // terms, all without their constant factors (render_bwd.cu); the conic is read before the
-    // record is cleared (the compiler cannot move loads of possibly aliasing memory past those
+    // the blend sums w dx and w dy (turned into the mean terms by the opacity and the conic here)
+    // and the conic terms (by the opacity), all without their constant factors (render_bwd.cu);
+    // the conic and opacity are read before the record is cleared (the compiler cannot move loads of possibly aliasing memory past those
     // stores)
     const float4 sa = __ldg(&p.splat[2 * idx]);  // {x, y, conic a, conic b}
-    const float conic_c = __ldg(&p.splat[2 * idx + 1].x);
+    const float4 sb = __ldg(&p.splat[2 * idx + 1]);  // {conic c, opacity, ...}
+    const float conic_c = sb.x, opacity = sb.y;
     const float4 z4 = make_float4(0.f, 0.f, 0.f, 0.f);
     p.grad_acc[3 * idx] = z4;
     p.grad_acc[3 * idx + 1] = z4;
     p.grad_acc[3 * idx + 2] = z4;
-    const float mx = fmaf(sa.z, g0.x, sa.w * g0.y), my = fmaf(sa.w, g0.x, conic_c * g0.y);
+    const float mx = opacity * fmaf(sa.z, g0.x, sa.w * g0.y), my = opacity * fmaf(sa.w, g0.x, conic_c * g0.y);
     const float dmean2D_x = -0.5f * (float)p.W * mx, dmean2D_y = -0.5f * (float)p.H * my;
-    const float3 dL_dconic = {-0.5f * g0.z, -0.5f * g0.w, -0.5f * g1.x};
+    const float ho = -0.5f * opacity;
+    const float3 dL_dconic = {ho * g0.z, ho * g0.w, ho * g1.x};
     dL_dcolor[0] = g1.z;
     dL_dcolor[1] = g1.w;
     dL_dcolor[2] = g2.x;

@@ -9,9 +9,10 @@
 // 1 - alpha serves both of the reference's divisions by it (relative error ~1e-7 per step, far
 // inside the gradients' 1e-3 tolerance).  The per-(pixel, splat) gradients (2 screen-space mean,
 // 3 conic, 1 opacity, 3 colour) are not pushed with 9 global atomics per pixel as in the
-// reference (and the mean terms are summed as q dx and q dy without the conic, the mean and conic
-// terms without their constant factors -W/2, -H/2, -1/2: the backward preprocess applies those
-// per Gaussian): a thread first sums them over its two
+// reference (and the mean terms are summed as w dx and w dy with w = G dL/dalpha, without the
+// opacity and the conic, the conic terms without the opacity, all without their constant factors
+// -W/2, -H/2, -1/2: the backward preprocess applies those per Gaussian): a thread first sums them
+// over its two
 // pixels and writes the 9 sums to its warp's shared buffer; every second contributing splat the
 // warp that owns the 8 x 8 patch reduces the buffer transposed (one lane per splat and value, 32
 // terms each) and adds the accumulator records with one atomic per value.  Warps skip splats
@@ -106,7 +107,7 @@ __device__ __forceinline__ void blend_backward_tile(const TileJob& job, const Bl
     for (int ch = 0; ch < 3; ++ch) dp[ch][i] = in ? job.dL_dpix[ch * HW + pix] : 0.f;
   }
   const float2 T_final = make_float2(Tf[0], Tf[1]);
-  const float2 neg_T_final = make_float2(-Tf[0], -Tf[1]);
+  const float2 neg_T_final = make_float2(-Tf[0], -Tf[1]);  // (folded into neg_T_bg below)
   float2 T = T_final;
   const float2 dp0 = make_float2(dp[0][0], dp[0][1]);
   const float2 dp1 = make_float2(dp[1][0], dp[1][1]);
@@ -115,6 +116,7 @@ __device__ __forceinline__ void blend_backward_tile(const TileJob& job, const Bl
   bgdot = fma2(f2(job.bg[0]), dp0, bgdot);
   bgdot = fma2(f2(job.bg[1]), dp1, bgdot);
   bgdot = fma2(f2(job.bg[2]), dp2, bgdot);
+  const float2 neg_T_bg = mul2(neg_T_final, bgdot);
   // colour of everything behind the current splat, accumulated back to front
   float2 acc0 = make_float2(0.f, 0.f), acc1 = acc0, acc2 = acc0;
   const float2 pyf = make_float2(patch.pyf(0), patch.pyf(1));
@@ -180,16 +182,17 @@ __device__ __forceinline__ void blend_backward_tile(const TileJob& job, const Bl
             acc1 = fma2(ae, e1, acc1);
             acc2 = fma2(ae, e2, acc2);
             dLda = mul2(dLda, T);
-            dLda = fma2(mul2(neg_T_final, inv), bgdot, dLda);
+            dLda = fma2(neg_T_bg, inv, dLda);  // the background term -T_final / (1 - alpha) bg.dL/dpix
             // With q = G dL/dG = o G dL/dalpha and the conic (a, b, c):
             //   dL/d(delta x) = -q (a dx + b dy), dL/d(delta y) = -q (c dy + b dx),
             //   dL/d(conic) = -q (dx^2, dx dy, dy^2) / 2.
-            // The per-pixel sums keep only q dx, q dy, q dx^2, ...: the conic (constant over the
-            // Gaussian's pixels) and the constant factors -W/2, -H/2 and -1/2 are applied once per
-            // Gaussian by the backward preprocess.  The thread's two pixels share dx, so the sums
-            // over them factor through sum q, sum q dy and sum q dy^2.
+            // The per-pixel sums keep only w dx, w dy, w dx^2, ... with w = G dL/dalpha = q / o:
+            // the opacity and the conic (constant over the Gaussian's pixels) and the constant
+            // factors -W/2, -H/2 and -1/2 are applied once per Gaussian by the backward
+            // preprocess.  The thread's two pixels share dx, so the sums over them factor through
+            // sum w, sum w dy and sum w dy^2.
             const float2 w5 = mul2(Ge, dLda);
-            const float2 q = mul2(f2(b.y), w5);
+            const float2 q = w5;
             const float2 qy = mul2(q, dy);
             const float qs = q.x + q.y, qdy = qy.x + qy.y;
             v[0] = dx * qs;
