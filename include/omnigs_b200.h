@@ -287,7 +287,7 @@ int omnigs_batch_backward(const OmnigsBatchArgs* args, const OmnigsBatchGrads* g
                           omnigs_stream_t stream);
 
 /* Splats staged per shared-memory batch in the blend kernels, per direction: 128, 256 or 512
- * (defaults: 256 forward, 128 backward).  Results do not depend on it (every pixel meets the same splats in the same order);
+ * (defaults: 128 forward, 128 backward).  Results do not depend on it (every pixel meets the same splats in the same order);
  * the best size depends on the scene and resolution.  Process-wide setting. */
 int omnigs_set_blend_batch(int forward, int backward);
 int omnigs_get_blend_batch(int* forward, int* backward);

@@ -252,10 +252,10 @@ void launch_duplicate(const DuplicateParams& p, cudaStream_t s);
 void launch_ranges(const RangesParams& p, cudaStream_t s);
 // Splats staged per shared-memory batch in the blend kernels: a template parameter chosen at run
 // time per direction (128, 256 or 512; set by omnigs_set_blend_batch or the autotuner).  Results
-// do not depend on it: every pixel meets the same splats in the same order.  Defaults: 256 for the
-// forward, 128 for the backward (the faster of the three for each on the 1M-Gaussian 2048x1024 view
-// on a B200: forward 0.625 vs 0.692 ms at 128, backward 1.149 vs 1.163 ms at 256).
-constexpr int kDefaultBatch = 256;
+// do not depend on it: every pixel meets the same splats in the same order.  Defaults: 128 for both
+// directions (the faster of the three for each on the 1M-Gaussian 2048x1024 view on a B200:
+// forward 0.512 vs 0.522 ms at 256, backward 1.149 vs 1.163 ms at 256).
+constexpr int kDefaultBatch = 128;
 constexpr int kDefaultBwdBatch = 128;
 int blend_batch_size(bool backward);
 

@@ -212,7 +212,7 @@ def test_blend_batch_sizes_and_autotuner(cuda):
         for k in ("dL_dmeans3D", "dL_dsh", "dL_dopacity", "dL_dscales", "dL_drotations"):
             assert _rel(getattr(grads, k), getattr(out[256][1], k)) < GRAD_RTOL, k
     finally:
-        batch.set_blend_batch(256, 128)  # the library's defaults
+        batch.set_blend_batch(128, 128)  # the library's defaults
 
 
 def test_batch_edge_cases(cuda):

@@ -280,12 +280,12 @@ def test_adam_validation():
 
 def test_blend_batch_setting():
     from omnigs_b200 import batch
-    assert batch.get_blend_batch() == (256, 128)  # the library's defaults
+    assert batch.get_blend_batch() == (128, 128)  # the library's defaults
     with pytest.raises(capi.OmnigsError):
         batch.set_blend_batch(100, 256)
     batch.set_blend_batch(128, 512)
     assert batch.get_blend_batch() == (128, 512)
-    batch.set_blend_batch(256, 128)
+    batch.set_blend_batch(128, 128)  # back to the library's defaults
     a, keep = _fake_batch()
     r = capi.TuneResult()
     assert capi.lib().omnigs_batch_autotune(ctypes.byref(a), 0x10000, 1 << 40, 0x10000, 1 << 40, 0,
