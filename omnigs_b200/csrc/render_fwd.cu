@@ -50,7 +50,10 @@ __device__ __forceinline__ void blend_forward_tile(const TileJob& job, const Ble
 
 // One view: block (x, y) blends tile (x, y).
 template <int kBatch>
-__global__ void __launch_bounds__(kBlendThreads) render_forward_kernel(RenderParams p) {
+// Twelve resident blocks per SM (at most 40 registers) measured fastest for the single-view kernel
+// on a B200 (0.511 -> 0.491 ms per 1M-Gaussian 2048x1024 view); the batched kernel measured
+// marginally slower under the same bound and keeps the compiler's choice.
+__global__ void __launch_bounds__(kBlendThreads, 12) render_forward_kernel(RenderParams p) {
   TileJob job;
   job.tile_x = blockIdx.x;
   job.tile_y = blockIdx.y;
