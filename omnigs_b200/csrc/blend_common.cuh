@@ -196,8 +196,8 @@ __device__ __forceinline__ void forward_pass(const TileJob& job, const BlendSour
     bool warp_done = __all_sync(kFullMask, done0 && done1);
     for (int k = 0; k * 32 < cnt && !warp_done; ++k) {
       const int j = k * 32 + lane;
-      // evaluated by every lane (slots past cnt hold stale splats, which j < cnt drops): measured
-      // 2 % faster than a branch around the test
+      // evaluated by every lane (slots past cnt hold stale or unset data, which j < cnt drops):
+      // measured 2 % faster than a branch around the test
       const bool hit = patch.template hit<kWrap>(s_a[j], s_b[j]) && j < cnt;
       unsigned m = __ballot_sync(kFullMask, hit);
       while (m) {
