@@ -117,8 +117,9 @@ __device__ __forceinline__ void blend_backward_tile(const TileJob& job, const Bl
   bgdot = fma2(f2(job.bg[1]), dp1, bgdot);
   bgdot = fma2(f2(job.bg[2]), dp2, bgdot);
   const float2 neg_T_bg = mul2(neg_T_final, bgdot);
-  // colour of everything behind the current splat, accumulated back to front
-  float2 acc0 = make_float2(0.f, 0.f), acc1 = acc0, acc2 = acc0;
+  // the colour of everything behind the current splat, accumulated back to front, enters the
+  // gradients only through its dot product with dL/dpix: that product is accumulated instead
+  float2 acc_dp = make_float2(0.f, 0.f);
   const float2 pyf = make_float2(patch.pyf(0), patch.pyf(1));
 
   float(*red)[kRedStride] = s_red[threadIdx.x >> 5];
@@ -176,14 +177,13 @@ __device__ __forceinline__ void blend_backward_tile(const TileJob& job, const Bl
             T = mul2(T, inv);  // transmittance in front of this splat
             const float2 dcd = mul2(ae, T);
             const float4 cv = s_c[jj];
-            // colour of this splat minus the colour behind it, per channel
-            const float2 e0 = sub2(f2(cv.x), acc0), e1 = sub2(f2(cv.y), acc1), e2 = sub2(f2(cv.z), acc2);
-            float2 dLda = mul2(e0, dp0);
-            dLda = fma2(e1, dp1, dLda);
-            dLda = fma2(e2, dp2, dLda);
-            acc0 = fma2(ae, e0, acc0);  // alpha c + (1 - alpha) acc
-            acc1 = fma2(ae, e1, acc1);
-            acc2 = fma2(ae, e2, acc2);
+            // (this splat's colour minus the colour behind it) . dL/dpix; the colour behind becomes
+            // alpha c + (1 - alpha) acc, so its product with dL/dpix grows by alpha times this
+            float2 c_dp = mul2(f2(cv.x), dp0);
+            c_dp = fma2(f2(cv.y), dp1, c_dp);
+            c_dp = fma2(f2(cv.z), dp2, c_dp);
+            float2 dLda = sub2(c_dp, acc_dp);
+            acc_dp = fma2(ae, dLda, acc_dp);
             dLda = mul2(dLda, T);
             dLda = fma2(neg_T_bg, inv, dLda);  // the background term -T_final / (1 - alpha) bg.dL/dpix
             // With q = G dL/dG = o G dL/dalpha and the conic (a, b, c):
